@@ -1,0 +1,419 @@
+// Oracle (test infrastructure only): a CPU restatement of the reference's host-side
+// BVH builder for the GPU path tracer.  Only tests/, __graft_entry__.smoke() and
+// bench.py's cpu_baseline leg may load this code; the product never does.
+//
+// Restated from the reference (paths relative to the reference project,
+// gfxlab/ = src/xyz/marsavic/gfxlab/):
+//   * primitive bounds      gfxlab/gpu/GpuScene.java:626-649, 840-903
+//                           (spheres from float centre +/- float radius, boxes from the
+//                           packed float corners, affines from the float-cast bounds; each
+//                           widened by two float ulps: nextDown2 / nextUp2)
+//   * centroid              gfxlab/gpu/GpuScene.java:78-80   ((min + max) * 0.5 in double)
+//   * BvhBuildState.build   gfxlab/gpu/GpuScene.java:1424-1447
+//   * bestSplit             gfxlab/gpu/GpuScene.java:1453-1488  (full sweep on every axis
+//                           whose centroid extent exceeds 1e-12; sort key (centroid, order)
+//                           with Double.compare; sequential prefix/suffix weight sums;
+//                           strict '<' keeps the first minimum)
+//   * weights               gfxlab/gpu/BvhBuildConfig.java:66-69  (q = 1 + lambda (c - 1))
+//   * per-type forest       gfxlab/gpu/GpuScene.java:702-720
+//   * flattenBvh / leafKind gfxlab/gpu/GpuScene.java:772-808   (preorder)
+//   * SAH statistics        gfxlab/gpu/GpuScene.java:810-838
+// Arithmetic is IEEE double with no contraction (Java strictfp semantics); this file
+// must be compiled with -ffp-contract=off.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+namespace {
+
+constexpr int REF_TYPE_MASK = (int)0xC0000000u;
+constexpr int REF_TYPE_SPHERE = 0x00000000;
+constexpr int REF_TYPE_BOX = 0x40000000;
+constexpr int REF_TYPE_AFFINE_SPHERE = (int)0x80000000u;
+constexpr int REF_TYPE_AFFINE_BOX = (int)0xC0000000u;
+
+struct Aabb {
+  double mn[3], mx[3];
+};
+
+inline double surface_area(const Aabb& b) {
+  double dx = b.mx[0] - b.mn[0];
+  double dy = b.mx[1] - b.mn[1];
+  double dz = b.mx[2] - b.mn[2];
+  double a = dx * dy;
+  double c = dx * dz;
+  double s = a + c;
+  double e = dy * dz;
+  s = s + e;
+  return 2.0 * s;
+}
+
+inline Aabb unite(const Aabb& a, const Aabb& b) {
+  Aabb r;
+  for (int k = 0; k < 3; ++k) {
+    r.mn[k] = std::min(a.mn[k], b.mn[k]);
+    r.mx[k] = std::max(a.mx[k], b.mx[k]);
+  }
+  return r;
+}
+
+struct Prim {
+  int ref;
+  int order;
+  Aabb bounds;
+  double cen[3];
+  double measured;  // c_i, the raw per-type weight
+};
+
+// Double.compare semantics for finite values (-0.0 orders before +0.0).
+inline int java_double_compare(double a, double b) {
+  if (a < b) return -1;
+  if (a > b) return 1;
+  int64_t ia, ib;
+  std::memcpy(&ia, &a, 8);
+  std::memcpy(&ib, &b, 8);
+  return ia == ib ? 0 : (ia < ib ? -1 : 1);
+}
+
+inline float next_down2(float v) { return std::nextafter(std::nextafter(v, -INFINITY), -INFINITY); }
+inline float next_up2(float v) { return std::nextafter(std::nextafter(v, INFINITY), INFINITY); }
+
+struct Node {
+  Aabb bounds;
+  int left = -1, right = -1;  // indices into the node pool, -1 for leaves
+  int start = -1, end = -1;
+};
+
+struct Config {
+  int weighted;
+  int leaf_size;
+  double traversal;
+  double lambda;
+};
+
+struct Builder {
+  std::vector<Prim>& prims;
+  const Config& cfg;
+  std::vector<Node> pool;
+
+  Builder(std::vector<Prim>& p, const Config& c) : prims(p), cfg(c) {}
+
+  double objective(const Prim& p) const {
+    if (!cfg.weighted) return 1.0;
+    double t = p.measured - 1.0;
+    t = cfg.lambda * t;
+    return 1.0 + t;
+  }
+
+  int make_leaf(const Aabb& b, int s, int e) {
+    Node n;
+    n.bounds = b;
+    n.start = s;
+    n.end = e;
+    pool.push_back(n);
+    return (int)pool.size() - 1;
+  }
+
+  struct Split {
+    bool valid = false;
+    std::vector<Prim> sorted;
+    int left_count = 0;
+    double cost = 0.0;
+  };
+
+  Split best_split(int start, int end, const Aabb& bounds, const Aabb& cb) {
+    int count = end - start;
+    double node_area = surface_area(bounds);
+    Split best;
+    std::vector<Aabb> prefix(count), suffix(count);
+    std::vector<double> pw(count), sw(count);
+    for (int axis = 0; axis < 3; ++axis) {
+      if (!(cb.mx[axis] - cb.mn[axis] > 1.0e-12)) continue;
+      std::vector<Prim> sorted(prims.begin() + start, prims.begin() + end);
+      std::stable_sort(sorted.begin(), sorted.end(), [axis](const Prim& a, const Prim& b) {
+        int c = java_double_compare(a.cen[axis], b.cen[axis]);
+        if (c != 0) return c < 0;
+        return a.order < b.order;
+      });
+      prefix[0] = sorted[0].bounds;
+      pw[0] = objective(sorted[0]);
+      for (int i = 1; i < count; ++i) {
+        prefix[i] = unite(prefix[i - 1], sorted[i].bounds);
+        pw[i] = pw[i - 1] + objective(sorted[i]);
+      }
+      suffix[count - 1] = sorted[count - 1].bounds;
+      sw[count - 1] = objective(sorted[count - 1]);
+      for (int i = count - 2; i >= 0; --i) {
+        suffix[i] = unite(suffix[i + 1], sorted[i].bounds);
+        sw[i] = sw[i + 1] + objective(sorted[i]);
+      }
+      bool improved = false;
+      int best_i = 0;
+      double best_cost = best.valid ? best.cost : 0.0;
+      bool have = best.valid;
+      for (int i = 1; i < count; ++i) {
+        double a = node_area * cfg.traversal;
+        double b = surface_area(prefix[i - 1]) * pw[i - 1];
+        double c = surface_area(suffix[i]) * sw[i];
+        double cost = (a + b) + c;
+        if (!have || cost < best_cost) {
+          have = true;
+          best_cost = cost;
+          best_i = i;
+          improved = true;
+        }
+      }
+      if (improved) {
+        best.valid = true;
+        best.cost = best_cost;
+        best.left_count = best_i;
+        best.sorted = std::move(sorted);
+      }
+    }
+    return best;
+  }
+
+  int build(int start, int end) {
+    Aabb bounds = prims[start].bounds;
+    Aabb cb;
+    for (int k = 0; k < 3; ++k) cb.mn[k] = cb.mx[k] = prims[start].cen[k];
+    for (int i = start + 1; i < end; ++i) {
+      bounds = unite(bounds, prims[i].bounds);
+      for (int k = 0; k < 3; ++k) {
+        cb.mn[k] = std::min(cb.mn[k], prims[i].cen[k]);
+        cb.mx[k] = std::max(cb.mx[k], prims[i].cen[k]);
+      }
+    }
+    int count = end - start;
+    if (count == 1) return make_leaf(bounds, start, end);
+    Split split = best_split(start, end, bounds, cb);
+    if (!split.valid) return make_leaf(bounds, start, end);
+    double wsum = 0.0;
+    for (int i = start; i < end; ++i) wsum += objective(prims[i]);
+    double leaf_cost = surface_area(bounds) * wsum;
+    if (count <= cfg.leaf_size && !(split.cost < leaf_cost)) return make_leaf(bounds, start, end);
+    std::copy(split.sorted.begin(), split.sorted.end(), prims.begin() + start);
+    int mid = start + split.left_count;
+    int l = build(start, mid);
+    int r = build(mid, end);
+    Node n;
+    n.bounds = bounds;
+    n.left = l;
+    n.right = r;
+    pool.push_back(n);
+    return (int)pool.size() - 1;
+  }
+};
+
+struct Summary {
+  int nodes = 0, leaves = 0, max_depth = 0, min_leaf = INT32_MAX, max_leaf = 0;
+};
+
+void summarize(const std::vector<Node>& pool, int n, int depth, Summary& s) {
+  s.nodes++;
+  s.max_depth = std::max(s.max_depth, depth);
+  const Node& nd = pool[n];
+  if (nd.left < 0) {
+    int occ = nd.end - nd.start;
+    s.leaves++;
+    s.min_leaf = std::min(s.min_leaf, occ);
+    s.max_leaf = std::max(s.max_leaf, occ);
+    return;
+  }
+  summarize(pool, nd.left, depth + 1, s);
+  summarize(pool, nd.right, depth + 1, s);
+}
+
+int leaf_kind(const std::vector<Prim>& p, int s, int e) {
+  int type = p[s].ref & REF_TYPE_MASK;
+  for (int i = s + 1; i < e; ++i)
+    if ((p[i].ref & REF_TYPE_MASK) != type) return -1;
+  switch (type) {
+    case REF_TYPE_SPHERE: return -2;
+    case REF_TYPE_BOX: return -3;
+    case REF_TYPE_AFFINE_SPHERE: return -4;
+    default: return -5;
+  }
+}
+
+struct Flat {
+  float* bounds;
+  int* data;
+  int* refs;
+  int next_node = 0;
+  int next_ref = 0;
+};
+
+int flatten(const std::vector<Node>& pool, int n, const std::vector<Prim>& p, Flat& f) {
+  int index = f.next_node++;
+  const Node& nd = pool[n];
+  for (int k = 0; k < 3; ++k) {
+    f.bounds[index * 6 + k] = (float)nd.bounds.mn[k];
+    f.bounds[index * 6 + 3 + k] = (float)nd.bounds.mx[k];
+  }
+  int* d = f.data + index * 4;
+  if (nd.left < 0) {
+    d[0] = leaf_kind(p, nd.start, nd.end);
+    d[1] = -1;
+    d[2] = f.next_ref;
+    d[3] = nd.end - nd.start;
+    for (int i = nd.start; i < nd.end; ++i) f.refs[f.next_ref++] = p[i].ref;
+    return index;
+  }
+  int l = flatten(pool, nd.left, p, f);
+  int r = flatten(pool, nd.right, p, f);
+  d[0] = l;
+  d[1] = r;
+  d[2] = -1;
+  d[3] = 0;
+  return index;
+}
+
+// sahCost / constructionSahCost (GpuScene.java:810-838).  mode 0: unit weights,
+// 1: measured weights, 2: construction weights.
+double sah_cost(const std::vector<Node>& pool, int n, const std::vector<Prim>& p, int mode,
+                const Builder& b) {
+  const Node& nd = pool[n];
+  if (nd.left < 0) {
+    double c = 0.0;
+    for (int i = nd.start; i < nd.end; ++i)
+      c += mode == 0 ? 1.0 : (mode == 1 ? p[i].measured : b.objective(p[i]));
+    return c;
+  }
+  double area = surface_area(nd.bounds);
+  if (!(area > 0.0)) return sah_cost(pool, nd.left, p, mode, b) + sah_cost(pool, nd.right, p, mode, b);
+  double l = surface_area(pool[nd.left].bounds) / area * sah_cost(pool, nd.left, p, mode, b);
+  double r = surface_area(pool[nd.right].bounds) / area * sah_cost(pool, nd.right, p, mode, b);
+  return (b.cfg.traversal + l) + r;
+}
+
+Aabb float_box(float x0, float y0, float z0, float x1, float y1, float z1) {
+  Aabb b;
+  b.mn[0] = next_down2(x0);
+  b.mn[1] = next_down2(y0);
+  b.mn[2] = next_down2(z0);
+  b.mx[0] = next_up2(x1);
+  b.mx[1] = next_up2(y1);
+  b.mx[2] = next_up2(z1);
+  return b;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Build configuration; mirrors gfxlab/gpu/BvhBuildConfig.java:6-15.  mode follows
+// BvhBuildMode ordinals (0 UNIFORM_SAH, 1 WEIGHTED_SAH, 2 PER_TYPE_SAH,
+// 3 PER_TYPE_WEIGHTED_SAH); the SBVH and rotation modes are not restated here.
+typedef struct {
+  int mode;
+  int leaf_size;
+  double traversal_weight;
+  double sphere_weight, box_weight, affine_sphere_weight, affine_box_weight;
+  double lambda;
+} orc_build_config;
+
+// Outputs must hold 2*N nodes (6 floats / 4 ints each), N refs and 4 roots, with
+// N = ns + nb + nas + nab.  counts: node_count, root_count, leaf_count, max_depth,
+// ref_count, min_leaf, max_leaf.  sah: generalized, uniform, weighted.
+// Returns 0 on success, negative on an unsupported configuration.
+int orc_build_bvh(const float* spheres, int ns, const float* boxes, int nb,
+                  const float* affine_sphere_bounds, int nas, const float* affine_box_bounds,
+                  int nab, const orc_build_config* cfg, float* node_bounds, int* node_data,
+                  int* refs, int* roots, int* counts, double* sah) {
+  if (cfg->mode < 0 || cfg->mode > 3 || cfg->leaf_size < 1) return -1;
+  bool weighted = cfg->mode == 1 || cfg->mode == 3;
+  bool per_type = cfg->mode >= 2;
+  Config c{weighted ? 1 : 0, cfg->leaf_size, cfg->traversal_weight,
+           weighted ? cfg->lambda : 0.0};
+  int total = ns + nb + nas + nab;
+  std::memset(counts, 0, 7 * sizeof(int));
+  sah[0] = sah[1] = sah[2] = 0.0;
+  if (total == 0) return 0;
+  std::vector<Prim> all;
+  all.reserve(total);
+  int order = 0;
+  for (int i = 0; i < ns; ++i, ++order) {
+    const float* s = spheres + 5 * i;
+    float cx = s[0], cy = s[1], cz = s[2], r = s[3];
+    Prim p{};
+    p.ref = REF_TYPE_SPHERE | i;
+    p.order = order;
+    p.bounds = float_box(cx - r, cy - r, cz - r, cx + r, cy + r, cz + r);
+    p.measured = cfg->sphere_weight;
+    all.push_back(p);
+  }
+  for (int i = 0; i < nb; ++i, ++order) {
+    const float* b = boxes + 7 * i;
+    Prim p{};
+    p.ref = REF_TYPE_BOX | i;
+    p.order = order;
+    p.bounds = float_box(b[0], b[1], b[2], b[3], b[4], b[5]);
+    p.measured = cfg->box_weight;
+    all.push_back(p);
+  }
+  for (int i = 0; i < nas; ++i, ++order) {
+    const float* b = affine_sphere_bounds + 6 * i;
+    Prim p{};
+    p.ref = REF_TYPE_AFFINE_SPHERE | i;
+    p.order = order;
+    p.bounds = float_box(b[0], b[1], b[2], b[3], b[4], b[5]);
+    p.measured = cfg->affine_sphere_weight;
+    all.push_back(p);
+  }
+  for (int i = 0; i < nab; ++i, ++order) {
+    const float* b = affine_box_bounds + 6 * i;
+    Prim p{};
+    p.ref = REF_TYPE_AFFINE_BOX | i;
+    p.order = order;
+    p.bounds = float_box(b[0], b[1], b[2], b[3], b[4], b[5]);
+    p.measured = cfg->affine_box_weight;
+    all.push_back(p);
+  }
+  for (auto& p : all)
+    for (int k = 0; k < 3; ++k) p.cen[k] = (p.bounds.mn[k] + p.bounds.mx[k]) * 0.5;
+
+  std::vector<std::vector<Prim>> parts;
+  if (per_type) {
+    for (int type : {REF_TYPE_SPHERE, REF_TYPE_BOX, REF_TYPE_AFFINE_SPHERE, REF_TYPE_AFFINE_BOX}) {
+      std::vector<Prim> part;
+      for (auto& p : all)
+        if ((p.ref & REF_TYPE_MASK) == type) part.push_back(p);
+      if (!part.empty()) parts.push_back(std::move(part));
+    }
+  } else {
+    parts.push_back(all);
+  }
+  Flat f{node_bounds, node_data, refs};
+  Summary total_summary;
+  int min_leaf = INT32_MAX, max_leaf = 0, max_depth = 0;
+  for (size_t t = 0; t < parts.size(); ++t) {
+    Builder b(parts[t], c);
+    b.pool.reserve(2 * parts[t].size());
+    int root = b.build(0, (int)parts[t].size());
+    Summary s;
+    summarize(b.pool, root, 0, s);
+    total_summary.nodes += s.nodes;
+    total_summary.leaves += s.leaves;
+    max_depth = std::max(max_depth, s.max_depth);
+    min_leaf = std::min(min_leaf, s.min_leaf);
+    max_leaf = std::max(max_leaf, s.max_leaf);
+    roots[t] = flatten(b.pool, root, parts[t], f);
+    sah[1] += sah_cost(b.pool, root, parts[t], 0, b);
+    sah[2] += sah_cost(b.pool, root, parts[t], 1, b);
+    sah[0] += sah_cost(b.pool, root, parts[t], 2, b);
+  }
+  counts[0] = total_summary.nodes;
+  counts[1] = (int)parts.size();
+  counts[2] = total_summary.leaves;
+  counts[3] = max_depth;
+  counts[4] = f.next_ref;
+  counts[5] = min_leaf == INT32_MAX ? 0 : min_leaf;
+  counts[6] = max_leaf;
+  if (total_summary.nodes != 2 * total_summary.leaves - (int)parts.size()) return -2;
+  return 0;
+}
+
+}  // extern "C"
