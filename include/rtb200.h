@@ -1,0 +1,183 @@
+/* rtb200 -- B200-native path tracer over cost-weighted SAH BVHs of analytic primitives.
+ *
+ * C ABI of librtb200.so: the drop-in boundary for the reference's CUDA render path.
+ * Reference paths are relative to the reference project; gfxlab/ stands for
+ * src/xyz/marsavic/gfxlab/.
+ *
+ * Conventions (mirroring gfxlab/gpu/GpuRayTracer.java):
+ *  - every call returns an rtb_status; nothing throws, traps or aborts;
+ *  - host buffers are owned by the caller; device memory is owned by the library;
+ *  - a context serialises its calls with its own mutex (the reference synchronises every
+ *    public method on the tracer, GpuRayTracer.java:339,445,601) and may be used from
+ *    any thread;
+ *  - the packed float layouts are exactly those of gfxlab/gpu/GpuScene.java:23-31
+ *    (sphere 5, box 7, plane 26, affine sphere / affine box 22, material 13 floats), so
+ *    a Java caller passes GpuScene.sphereData() and friends unchanged.
+ */
+#ifndef RTB200_H
+#define RTB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RTB_API __attribute__((visibility("default")))
+#else
+#define RTB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  RTB_OK = 0,
+  RTB_ERR_INVALID_ARGUMENT = 1, /* IllegalArgumentException in the reference */
+  RTB_ERR_UNAVAILABLE = 2,      /* no usable device (GpuRayTracer.isAvailable() false) */
+  RTB_ERR_CUDA = 3,             /* a CUDA runtime call failed; see rtb_last_error */
+  RTB_ERR_OUT_OF_MEMORY = 4,
+  RTB_ERR_UNSUPPORTED = 5,      /* a build mode this library does not implement */
+  RTB_ERR_DEVICE_CHECK = 6,     /* a kernel's own bounds / input check failed */
+  RTB_ERR_WATCHDOG = 7,         /* a kernel gave up at its work budget or was aborted
+                                   (IllegalStateException in GpuRayTracer.java:572-580) */
+  RTB_ERR_LIMIT = 8             /* a documented size limit was exceeded */
+} rtb_status;
+
+typedef struct rtb_context rtb_context;
+typedef struct rtb_scene rtb_scene;
+
+/* Scene payload in the reference's packed layouts (GpuScene.java:507-601).  The affine
+ * bounds are the float-cast world bounds GpuScene keeps beside each affine record
+ * (GpuScene.java:640-649); they are only read by rtb_scene_build. */
+typedef struct {
+  const float* spheres;        int sphere_count;        /* 5 floats: centre, radius, material */
+  const float* boxes;          int box_count;           /* 7 floats: min, max, material */
+  const float* planes;         int plane_count;         /* 26 floats (GpuScene.planeData) */
+  const float* affine_spheres; int affine_sphere_count; /* 22 floats */
+  const float* affine_boxes;   int affine_box_count;    /* 22 floats */
+  const float* materials;      int material_count;      /* 13 floats */
+  const float* affine_sphere_bounds;                    /* 6 floats: min.xyz, max.xyz */
+  const float* affine_box_bounds;                       /* 6 floats */
+  float background[3];
+} rtb_scene_desc;
+
+/* A flattened BVH as GpuScene.bvhNodeBoundsData / bvhNodeData / bvhPrimitiveRefs /
+ * bvhRootIndices produce it (GpuScene.java:30-31, 772-808). */
+typedef struct {
+  const float* node_bounds;  /* 6 floats per node */
+  const int* node_data;      /* 4 ints per node: left|kind, right, first ref, count */
+  int node_count;
+  const int* primitive_refs; /* type << 30 | index */
+  int primitive_ref_count;
+  const int* root_indices;   /* 1..4 roots */
+  int root_count;
+} rtb_bvh_desc;
+
+/* BvhBuildConfig (gfxlab/gpu/BvhBuildConfig.java:6-15); mode is a BvhBuildMode ordinal
+ * (0 UNIFORM_SAH, 1 WEIGHTED_SAH, 2 PER_TYPE_SAH, 3 PER_TYPE_WEIGHTED_SAH; the SBVH and
+ * rotation modes return RTB_ERR_UNSUPPORTED). */
+typedef struct {
+  int mode;
+  int leaf_size;
+  double traversal_weight;
+  double sphere_weight, box_weight, affine_sphere_weight, affine_box_weight;
+  double lambda;
+} rtb_build_config;
+
+/* GpuScene.BvhStats (GpuScene.java:113-133) plus the device build time. */
+typedef struct {
+  int node_count, root_count, leaf_count, max_depth, primitive_ref_count, leaf_size;
+  int min_leaf_occupancy, max_leaf_occupancy;
+  double generalized_sah_cost, uniform_sah_cost, weighted_sah_cost;
+  long long bytes;
+  double build_ms;          /* CUDA-event time of the device build */
+  int sequential_nodes;     /* nodes whose split needed the exact sequential weight order */
+} rtb_bvh_stats;
+
+/* GpuCamera (gfxlab/gpu/GpuCamera.java): direction = forward + right u + up v. */
+typedef struct {
+  float position[3], forward[3], right[3], up[3];
+} rtb_camera;
+
+/* Arguments of GpuRayTracer.renderSample (GpuRayTracer.java:317-432). */
+typedef struct {
+  int width, height;
+  int samples_per_frame;   /* >= 1 */
+  int max_depth;           /* [0, 32], GpuRayTracer.validateFullPathDepth */
+  int frame_index;
+  unsigned long long frame_seed;
+  int use_bvh;             /* 0: test every primitive (the reference's GPU_LINEAR) */
+  int collect_metrics;     /* count traversal work into rtb_frame_stats.counters */
+  int block_size;          /* 0: tuned default */
+} rtb_render_params;
+
+/* GpuRayTracer.FrameStats (GpuRayTracer.java:79-99).  counters follow the reference's
+ * STAT_* order (GpuKernelSources.java:30-43): rays, aabb tests, primitive tests, sphere,
+ * box, plane, affine sphere, affine box tests, stack overflows, max stack size, internal
+ * node visits, leaf visits, homogeneous leaf visits, mixed leaf visits. */
+typedef struct {
+  long long total_ns, kernel_ns, max_physical_kernel_ns, copy_ns, upload_ns;
+  long long counters[14];
+  int physical_launches;
+} rtb_frame_stats;
+
+/* ---- context (GpuRayTracer constructor / isAvailable / close, GpuRayTracer.java:256-287,
+ *      780-835, 1223-1310) ---- */
+RTB_API rtb_status rtb_context_create(int device, rtb_context** out);
+RTB_API rtb_status rtb_context_destroy(rtb_context* ctx);
+RTB_API const char* rtb_status_string(rtb_status status);
+/* Message of the last failed call on this context (empty when none). */
+RTB_API const char* rtb_last_error(const rtb_context* ctx);
+/* GpuRayTracer.deviceInfo (GpuRayTracer.java:308-310). */
+RTB_API rtb_status rtb_device_info(rtb_context* ctx, char* name, int name_len, int* cc_major,
+                           int* cc_minor, int* sm_count);
+
+/* ---- scenes (GpuRayTracer.ensureSceneResident / uploadScene, GpuRayTracer.java:873-948) ----
+ * rtb_scene_upload takes a caller-built BVH (or none: linear traversal only);
+ * rtb_scene_build builds the BVH on the device from the packed primitives
+ * (the GpuScene.buildBvhData step, GpuScene.java:614-700, moved onto the GPU). */
+RTB_API rtb_status rtb_scene_upload(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_bvh_desc* bvh,
+                            rtb_scene** out);
+RTB_API rtb_status rtb_scene_build(rtb_context* ctx, const rtb_scene_desc* desc,
+                           const rtb_build_config* config, rtb_scene** out, rtb_bvh_stats* stats);
+/* Copies the scene's BVH back in the reference's flattened layout (for topology hashes).
+ * Sizes come from rtb_scene_bvh_sizes. */
+RTB_API rtb_status rtb_scene_bvh_sizes(rtb_context* ctx, const rtb_scene* scene, int* node_count,
+                               int* ref_count, int* root_count);
+RTB_API rtb_status rtb_scene_download_bvh(rtb_context* ctx, const rtb_scene* scene, float* node_bounds,
+                                  int* node_data, int* refs, int* roots);
+RTB_API rtb_status rtb_scene_destroy(rtb_context* ctx, rtb_scene* scene);
+
+/* ---- queries ---- */
+/* GpuRayTracer.traceReplay (GpuRayTracer.java:593-716): closest hit of caller rays
+ * (origin.xyz, direction.xyz per ray, host memory).  Outputs are host arrays of
+ * ray_count entries (hit_normals: 3 per ray); misses give flag 0, distance +inf,
+ * order -1, material -1 and a zero normal. */
+RTB_API rtb_status rtb_trace_replay(rtb_context* ctx, rtb_scene* scene, const float* rays, int ray_count,
+                            int use_bvh, int collect_metrics, int* hit_flags,
+                            float* hit_distances, int* hit_orders, int* hit_materials,
+                            float* hit_normals);
+
+/* GpuRayTracer.renderSample (GpuRayTracer.java:317-432): renders samples_per_frame
+ * samples per pixel and writes the per-pixel mean (3 floats per pixel, row-major) to the
+ * host buffer rgb. */
+RTB_API rtb_status rtb_render_sample(rtb_context* ctx, rtb_scene* scene, const rtb_camera* camera,
+                             const rtb_render_params* params, float* rgb);
+
+/* Same frame into a caller-owned DEVICE buffer on a caller stream (cudaStream_t, or NULL
+ * for the context's stream); returns after the launch is queued. */
+RTB_API rtb_status rtb_render_device(rtb_context* ctx, rtb_scene* scene, const rtb_camera* camera,
+                             const rtb_render_params* params, float* rgb_device, void* stream);
+
+/* GpuRayTracer.lastFrameStats / lastPhysicalKernelLaunchCount (GpuRayTracer.java:294-306). */
+RTB_API rtb_status rtb_last_frame_stats(rtb_context* ctx, rtb_frame_stats* out);
+
+/* Host-writable abort: running persistent kernels of this context stop at their next
+ * work fetch and the call returns RTB_ERR_WATCHDOG.  Cleared by the next render call. */
+RTB_API rtb_status rtb_request_abort(rtb_context* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RTB200_H */

@@ -1,0 +1,76 @@
+// Host-side internals shared by the library's translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/rtb200.h"
+#include "rtb_device.cuh"
+
+struct rtb_context {
+  int device = 0;
+  int sm_count = 0;
+  int cc_major = 0, cc_minor = 0;
+  char name[256] = {0};
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::mutex mu;
+  std::string last_error;
+  rtb_frame_stats last{};
+  // Small device scratch: [0] pixel queue head (u64), [1..] status words, counters.
+  unsigned long long* d_work = nullptr;
+  int* d_abort = nullptr;  // host-written abort flag (device memory)
+  // Replay / output staging reused across calls.
+  void* d_stage = nullptr;
+  size_t stage_bytes = 0;
+  void* h_pinned = nullptr;
+  size_t pinned_bytes = 0;
+};
+
+struct rtb_scene {
+  // One arena holds every device array of the scene.
+  void* arena = nullptr;
+  size_t arena_bytes = 0;
+  rtb::DevScene dev{};
+  // Reference-layout BVH kept on the device for download (topology checks).
+  float* ref_node_bounds = nullptr;
+  int* ref_node_data = nullptr;
+  int* ref_refs = nullptr;
+  int* ref_roots = nullptr;
+  int ref_node_count = 0, ref_ref_count = 0, ref_root_count = 0;
+  bool has_bvh = false;
+  std::vector<void*> extra;  // additional allocations freed with the scene
+};
+
+namespace rtb {
+
+// Status helpers.
+rtb_status fail(rtb_context* ctx, rtb_status s, const std::string& msg);
+rtb_status cuda_fail(rtb_context* ctx, cudaError_t e, const char* what);
+
+// Device staging buffer of at least `bytes` (grown on demand, owned by the context).
+void* stage(rtb_context* ctx, size_t bytes);
+void* pinned(rtb_context* ctx, size_t bytes);
+
+// rtb_scene.cu
+rtb_status scene_create(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_bvh_desc* host_bvh,
+                        const float* d_node_bounds, const int* d_node_data, int node_count,
+                        const int* d_refs, int ref_count, const int* d_roots, int root_count,
+                        rtb_scene** out);
+void scene_free(rtb_scene* s);
+
+// rtb_render.cu
+rtb_status render_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
+                        const rtb_render_params* p, float* d_rgb, cudaStream_t stream,
+                        bool timed);
+rtb_status trace_rays(rtb_context* ctx, rtb_scene* scene, const float* d_rays, int n, int use_bvh,
+                      int collect_metrics, int* d_flags, float* d_t, int* d_order, int* d_mat,
+                      float* d_normal, cudaStream_t stream);
+
+// rtb_build.cu
+rtb_status build_bvh(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_build_config* cfg,
+                     rtb_scene** out, rtb_bvh_stats* stats);
+
+}  // namespace rtb

@@ -1,0 +1,312 @@
+// Path-tracing and closest-hit kernels.
+//
+// Render: one persistent launch per frame (the reference issues one launch per sample and
+// tile, GpuRayTracer.java:356-376).  Each resident thread owns one pixel at a time and runs
+// its samples in order, one path segment per loop iteration; a lane whose path ends starts
+// the next sample (or fetches the next pixel from a warp-aggregated queue) while the other
+// lanes continue, so warps stay full across uneven path lengths.  The per-pixel sum is the
+// reference's FP32 running sum over samples 0..spp-1 scaled by 1/spp after the last one
+// (GpuKernelSources.java:1284-1293), and each sample consumes the reference's random
+// stream (seed K:1231-1254, jitter and camera K:1256-1264, tracePath K:1061-1165), so the
+// image matches the reference's renderKernel bit for bit under the same arithmetic.
+#include "rtb_internal.h"
+
+namespace rtb {
+namespace {
+
+struct RenderArgs {
+  DevScene S;
+  float3 cam_pos, cam_f, cam_r, cam_u;
+  int width, height, spp, max_depth, frame_index;
+  unsigned long long frame_seed;
+  float* out;
+  long long pixels;
+  unsigned long long* queue;       // pixel queue head
+  int* abort_flag;                 // host-set abort
+  unsigned long long* counters;    // 14 counters (metrics build) + overflow count
+};
+
+__device__ __forceinline__ float luminance(float3 c) {  // K:181-183
+  return c.x * 0.212655f + c.y * 0.715158f + c.z * 0.072187f;
+}
+__device__ __forceinline__ float3 reflect_dir(float3 n, float3 i) {  // K:1022-1024
+  return sub(mul(n, 2.0f * dot(i, n)), i);
+}
+__device__ __forceinline__ float3 refract_dir(float3 incoming, float3 n, float eta) {  // K:1026-1039
+  float3 i = normalize_safe(incoming);
+  float c1 = dot(i, n);
+  float ri = (c1 >= 0.0f) ? eta : -1.0f / eta;
+  float inv_ri2 = 1.0f / (ri * ri);
+  float c2 = 1.0f - (1.0f - c1 * c1) * inv_ri2;
+  if (c2 <= 0.0f) return normalize_safe(reflect_dir(n, i));
+  float sq = sqrtf(c2);
+  return normalize_safe(sub(mul(n, c1 - sq * ri), i));
+}
+
+__device__ __forceinline__ uint32_t pixel_base_seed(unsigned long long frame_seed, int frame_index,
+                                                    uint32_t pixel) {  // K:1231-1236
+  uint32_t s = hash_u32((uint32_t)(frame_seed & 0xFFFFFFFFULL));
+  s ^= hash_u32((uint32_t)(frame_seed >> 32));
+  s ^= hash_u32((uint32_t)frame_index);
+  s ^= hash_u32(pixel);
+  return hash_u32(s);
+}
+
+template <bool METRICS>
+__global__ void __launch_bounds__(128) k_render(RenderArgs a) {
+  const DevScene& S = a.S;
+  const int lane = threadIdx.x & 31;
+  TraceCounters c{};
+  unsigned long long rays = 0;
+  // Per-lane state.
+  long long pixel = -1;
+  int x = 0, y = 0, so = 0;
+  uint32_t base_seed = 0, rng = 0;
+  float3 acc = v3(0, 0, 0), thr = v3(0, 0, 0), rad = v3(0, 0, 0), o = v3(0, 0, 0), d = v3(0, 0, 0);
+  int depth = 0;
+  bool path = false;
+  bool done = false;
+  const float aspect = (float)a.width / (float)a.height;
+  while (true) {
+    // ---- fetch a pixel (warp-aggregated) for lanes that need one
+    bool need = !done && pixel < 0;
+    unsigned need_mask = __ballot_sync(0xFFFFFFFFu, need);
+    if (need_mask) {
+      unsigned long long basep = 0;
+      int leader = __ffs(need_mask) - 1;
+      if (lane == leader) {
+        basep = (*(volatile int*)a.abort_flag) ? (unsigned long long)a.pixels
+                                               : atomicAdd(a.queue, (unsigned long long)__popc(need_mask));
+      }
+      basep = __shfl_sync(0xFFFFFFFFu, basep, leader);
+      if (need) {
+        long long p = (long long)basep + __popc(need_mask & ((1u << lane) - 1u));
+        if (p >= a.pixels) {
+          done = true;
+        } else {
+          pixel = p;
+          x = (int)(p % a.width);
+          y = (int)(p / a.width);
+          so = 0;
+          base_seed = pixel_base_seed(a.frame_seed, a.frame_index,
+                                      (uint32_t)y * (uint32_t)a.width + (uint32_t)x);
+        }
+      }
+    }
+    if (__all_sync(0xFFFFFFFFu, done)) break;
+    // ---- start a sample (renderKernel prologue, K:1251-1264)
+    if (!done && !path) {
+      uint32_t seed = base_seed ^ hash_u32((uint32_t)so);
+      seed ^= hash_u32((uint32_t)(so * 0x9E3779B9u));
+      rng = hash_u32(seed);
+      float jx = rand01(&rng) - 0.5f;
+      float jy = rand01(&rng) - 0.5f;
+      float u = ((((float)x + 0.5f) + jx) * (2.0f / (float)a.width) - 1.0f) * aspect;
+      float v = 1.0f - ((((float)y + 0.5f) + jy) * (2.0f / (float)a.height));
+      o = a.cam_pos;
+      d = add(add(a.cam_f, mul(a.cam_r, u)), mul(a.cam_u, v));
+      thr = v3(1.0f, 1.0f, 1.0f);
+      rad = v3(0.0f, 0.0f, 0.0f);
+      depth = 0;
+      path = a.max_depth > 0;
+    }
+    // ---- one path segment (tracePath loop body, K:1098-1162)
+    bool finished = !done && !path;  // max_depth == 0: the sample is black
+    if (!done && path) {
+      if (METRICS) rays++;
+      Best b;
+      bool hit = trace_closest<METRICS>(S, o, d, b, &c, nullptr);
+      if (!hit) {
+        rad = add(rad, mulv(thr, S.background));
+        finished = true;
+      } else {
+        float3 pos, n;
+        int mi;
+        hit_record(S, b, o, d, &pos, &n, &mi);
+        float4 m0 = make_float4(0, 0, 0, 0), m1 = m0, m2 = m0, m3 = m0;
+        if (mi >= 0) {
+          const float4* mp = S.materials + 4 * mi;
+          m0 = __ldg(mp);
+          m1 = __ldg(mp + 1);
+          m2 = __ldg(mp + 2);
+          m3 = __ldg(mp + 3);
+        }
+        float3 cd = v3(m0.x, m0.y, m0.z), cr = v3(m1.x, m1.y, m1.z), ct = v3(m2.x, m2.y, m2.z);
+        rad = add(rad, mulv(thr, v3(m3.x, m3.y, m3.z)));
+        float3 inc = neg(d);
+        float wd = luminance(cd), wr = luminance(cr), wt = luminance(ct);
+        float sum = wd + wr + wt;
+        if (sum <= 0.0f) {
+          finished = true;
+        } else {
+          float xi = rand01(&rng) * sum;
+          float3 nd, wc;
+          if (xi < wd) {
+            float pc = wd / sum;
+            float z = rand01(&rng) * 2.0f - 1.0f;
+            float t = rand01(&rng) * 2.0f * CUDART_PI_F;
+            float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+            nd = add(v3(r * cosf(t), r * sinf(t), z), n);
+            wc = divs(cd, pc);
+          } else if (xi < wd + wr) {
+            float pc = wr / sum;
+            nd = reflect_dir(n, inc);
+            wc = divs(cr, pc);
+          } else {
+            float pc = wt / sum;
+            nd = refract_dir(inc, n, m0.w);
+            wc = divs(ct, pc);
+          }
+          o = add(pos, mul(nd, kEps));
+          thr = mulv(thr, wc);
+          d = nd;
+          depth++;
+          if (depth >= a.max_depth) finished = true;
+        }
+      }
+    }
+    if (finished) {
+      path = false;
+      acc = so == 0 ? rad : add(acc, rad);
+      so++;
+      if (so == a.spp) {
+        acc = mul(acc, 1.0f / (float)a.spp);
+        float* out = a.out + 3 * pixel;
+        out[0] = acc.x;
+        out[1] = acc.y;
+        out[2] = acc.z;
+        pixel = -1;
+      }
+    }
+  }
+  if (METRICS) {
+    unsigned long long* k = a.counters;
+    atomicAdd(k + 0, rays);
+    atomicAdd(k + 1, c.aabb);
+    atomicAdd(k + 2, c.prim);
+    atomicAdd(k + 3, c.type[0]);
+    atomicAdd(k + 4, c.type[1]);
+    atomicAdd(k + 5, c.type[2]);
+    atomicAdd(k + 6, c.type[3]);
+    atomicAdd(k + 7, c.type[4]);
+    atomicAdd(k + 8, c.overflow);
+    atomicMax(k + 9, c.maxstack);
+    atomicAdd(k + 10, c.internal);
+    atomicAdd(k + 11, c.leaf);
+    atomicAdd(k + 12, c.homo);
+    atomicAdd(k + 13, c.mixed);
+  }
+}
+
+template <bool METRICS>
+__global__ void __launch_bounds__(256) k_trace(DevScene S, const float* rays, int n, int* flags,
+                                               float* dist, int* order, int* mat, float* normal,
+                                               unsigned long long* counters) {
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const float* ry = rays + 6 * (size_t)r;
+  float3 o = v3(ry[0], ry[1], ry[2]);
+  float3 d = v3(ry[3], ry[4], ry[5]);
+  TraceCounters c{};
+  Best b;
+  bool hit = trace_closest<METRICS>(S, o, d, b, &c, nullptr);
+  float3 pos, nn = v3(0, 0, 0);
+  int mi = -1;
+  if (hit) hit_record(S, b, o, d, &pos, &nn, &mi);
+  flags[r] = hit ? 1 : 0;
+  dist[r] = hit ? b.t : CUDART_INF_F;
+  order[r] = hit ? b.order : -1;
+  mat[r] = hit ? mi : -1;
+  normal[3 * (size_t)r] = nn.x;
+  normal[3 * (size_t)r + 1] = nn.y;
+  normal[3 * (size_t)r + 2] = nn.z;
+  if (METRICS) {
+    atomicAdd(counters + 0, 1ULL);
+    atomicAdd(counters + 1, c.aabb);
+    atomicAdd(counters + 2, c.prim);
+    atomicAdd(counters + 3, c.type[0]);
+    atomicAdd(counters + 4, c.type[1]);
+    atomicAdd(counters + 5, c.type[2]);
+    atomicAdd(counters + 6, c.type[3]);
+    atomicAdd(counters + 7, c.type[4]);
+    atomicAdd(counters + 8, c.overflow);
+    atomicMax(counters + 9, c.maxstack);
+    atomicAdd(counters + 10, c.internal);
+    atomicAdd(counters + 11, c.leaf);
+    atomicAdd(counters + 12, c.homo);
+    atomicAdd(counters + 13, c.mixed);
+  }
+}
+
+int g_render_blocks_per_sm[2] = {0, 0};
+
+}  // namespace
+
+rtb_status render_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
+                        const rtb_render_params* p, float* d_rgb, cudaStream_t stream, bool timed) {
+  if (!scene || !cam || !p || !d_rgb) return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "null argument");
+  if (p->width < 1 || p->height < 1 || p->samples_per_frame < 1)
+    return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "image size and samples must be positive");
+  if (p->max_depth < 0 || p->max_depth > 32)
+    return fail(ctx, RTB_ERR_INVALID_ARGUMENT,
+                "GPU full-path depth must be in [0, 32] but was " + std::to_string(p->max_depth));
+  RenderArgs a;
+  a.S = scene->dev;
+  a.S.use_bvh = (p->use_bvh && scene->has_bvh) ? 1 : 0;
+  a.cam_pos = make_float3(cam->position[0], cam->position[1], cam->position[2]);
+  a.cam_f = make_float3(cam->forward[0], cam->forward[1], cam->forward[2]);
+  a.cam_r = make_float3(cam->right[0], cam->right[1], cam->right[2]);
+  a.cam_u = make_float3(cam->up[0], cam->up[1], cam->up[2]);
+  a.width = p->width;
+  a.height = p->height;
+  a.spp = p->samples_per_frame;
+  a.max_depth = p->max_depth;
+  a.frame_index = p->frame_index;
+  a.frame_seed = p->frame_seed;
+  a.out = d_rgb;
+  a.pixels = (long long)p->width * p->height;
+  a.queue = ctx->d_work;
+  a.abort_flag = ctx->d_abort;
+  a.counters = ctx->d_work + 8;
+  cudaMemsetAsync(ctx->d_work, 0, 32 * sizeof(unsigned long long), stream);
+  int metrics = p->collect_metrics ? 1 : 0;
+  int& bps = g_render_blocks_per_sm[metrics];
+  if (bps == 0) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, metrics ? (const void*)k_render<true>
+                                                                : (const void*)k_render<false>,
+                                                  128, 0);
+    if (bps < 1) bps = 1;
+  }
+  long long want = (a.pixels + 127) / 128;
+  long long grid = std::min<long long>((long long)ctx->sm_count * bps, want);
+  if (timed) cudaEventRecord(ctx->ev0, stream);
+  if (metrics)
+    k_render<true><<<(unsigned)grid, 128, 0, stream>>>(a);
+  else
+    k_render<false><<<(unsigned)grid, 128, 0, stream>>>(a);
+  if (timed) cudaEventRecord(ctx->ev1, stream);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "render launch");
+  return RTB_OK;
+}
+
+rtb_status trace_rays(rtb_context* ctx, rtb_scene* scene, const float* d_rays, int n, int use_bvh,
+                      int collect_metrics, int* d_flags, float* d_t, int* d_order, int* d_mat,
+                      float* d_normal, cudaStream_t stream) {
+  DevScene S = scene->dev;
+  S.use_bvh = (use_bvh && scene->has_bvh) ? 1 : 0;
+  unsigned long long* counters = ctx->d_work + 8;
+  cudaMemsetAsync(ctx->d_work, 0, 32 * sizeof(unsigned long long), stream);
+  unsigned grid = (unsigned)((n + 255) / 256);
+  if (n > 0) {
+    if (collect_metrics)
+      k_trace<true><<<grid, 256, 0, stream>>>(S, d_rays, n, d_flags, d_t, d_order, d_mat, d_normal, counters);
+    else
+      k_trace<false><<<grid, 256, 0, stream>>>(S, d_rays, n, d_flags, d_t, d_order, d_mat, d_normal, counters);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "trace launch");
+  return RTB_OK;
+}
+
+}  // namespace rtb
