@@ -420,9 +420,15 @@ __device__ __forceinline__ void trace_leaf(const DevScene& S, int first, int met
 
 // Closest hit of one ray against the resident scene (traceClosest, K:963-1020): the BVH
 // (or every bounded primitive in linear mode), then the planes.  Returns true on a hit.
+//
+// Warp-cooperative: all 32 lanes of the warp call it together (lanes without a ray pass
+// active = false).  The traversal loop is warp-uniform -- each iteration every lane that
+// still has work processes one node (testing both child boxes and any leaf child
+// immediately) and the loop condition is a warp vote -- so divergent lanes reconverge once
+// per node instead of drifting apart for a whole traversal.
 template <bool METRICS>
-__device__ bool trace_closest(const DevScene& S, float3 o, float3 d, Best& b, TraceCounters* c,
-                              int* overflow_flag) {
+__device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active, Best& b,
+                              TraceCounters* c, int* overflow_flag) {
   b.t = 1e30f;
   b.order = 0x7FFFFFFF;
   b.type = -1;
@@ -434,68 +440,52 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, Best& b, Tr
     int stack[kStackSize];
     float estack[kStackSize];
     int sp = 0;
-    int node = 0;
+    int node = active ? 0 : -1;
     bool overflow = false;
     // A tree visits each node at most once per ray; the cap only matters for malformed
     // (cyclic) caller-supplied trees, which then take the exhaustive path below.
     int budget = S.node_count + 8;
-    while (true) {
-      if (--budget < 0) {
-        overflow = true;
-        break;
-      }
-      const float4* np = S.nodes + 4 * node;
-      float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2);
-      int4 n3 = __ldg(reinterpret_cast<const int4*>(np + 3));
-      float lim = prune_limit(b.t);
-      float e0 = child_entry(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, inv, lim);
-      float e1 = child_entry(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, inv, lim);
-      if (METRICS) {
-        c->internal++;
-        c->aabb += 2;
-      }
-      // Visit the nearer child first.
-      bool swap = e1 < e0;
-      float en = swap ? e1 : e0, ef = swap ? e0 : e1;
-      int ln = swap ? n3.y : n3.x, lf = swap ? n3.x : n3.y;
-      int mn = swap ? n3.w : n3.z, mf = swap ? n3.z : n3.w;
-      int next = -1;
-      if (en != CUDART_INF_F) {
-        if (ln < 0) {
-          trace_leaf<METRICS>(S, ~ln, mn, o, d, dd, b, c);
-        } else {
-          next = ln;
+    while (__any_sync(0xFFFFFFFFu, node >= 0)) {
+      if (node >= 0) {
+        const float4* np = S.nodes + 4 * node;
+        float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2);
+        int4 n3 = __ldg(reinterpret_cast<const int4*>(np + 3));
+        float lim = prune_limit(b.t);
+        float e0 = child_entry(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, inv, lim);
+        float e1 = child_entry(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, inv, lim);
+        if (METRICS) {
+          c->internal++;
+          c->aabb += 2;
         }
-      }
-      if (ef != CUDART_INF_F && ef <= prune_limit(b.t)) {
-        if (lf < 0) {
+        bool swap = e1 < e0;
+        float en = swap ? e1 : e0, ef = swap ? e0 : e1;
+        int ln = swap ? n3.y : n3.x, lf = swap ? n3.x : n3.y;
+        int mn = swap ? n3.w : n3.z, mf = swap ? n3.z : n3.w;
+        if (en != CUDART_INF_F && ln < 0) trace_leaf<METRICS>(S, ~ln, mn, o, d, dd, b, c);
+        if (ef != CUDART_INF_F && lf < 0 && ef <= prune_limit(b.t))
           trace_leaf<METRICS>(S, ~lf, mf, o, d, dd, b, c);
-        } else if (next < 0) {
-          next = lf;
-        } else if (sp < kStackSize) {
-          stack[sp] = lf;
-          estack[sp] = ef;
-          sp++;
-          if (METRICS && (unsigned long long)sp > c->maxstack) c->maxstack = sp;
-        } else {
-          overflow = true;
-          break;
+        int next = (en != CUDART_INF_F && ln >= 0) ? ln : -1;
+        if (ef != CUDART_INF_F && lf >= 0 && ef <= prune_limit(b.t)) {
+          if (next < 0) {
+            next = lf;
+          } else if (sp < kStackSize) {
+            stack[sp] = lf;
+            estack[sp] = ef;
+            sp++;
+            if (METRICS && (unsigned long long)sp > c->maxstack) c->maxstack = sp;
+          } else {
+            overflow = true;
+          }
         }
-      }
-      if (next >= 0) {
-        node = next;
-        continue;
-      }
-      // Pop the next subtree still closer than the current hit.
-      node = -1;
-      while (sp > 0) {
-        --sp;
-        if (estack[sp] <= prune_limit(b.t)) {
-          node = stack[sp];
-          break;
+        // Pop the next subtree still closer than the current hit.
+        float plim = prune_limit(b.t);
+        while (next < 0 && sp > 0) {
+          --sp;
+          if (estack[sp] <= plim) next = stack[sp];
         }
+        if (--budget < 0) overflow = true;
+        node = overflow ? -1 : next;
       }
-      if (node < 0) break;
     }
     if (overflow) {
       // A tree deeper than the stack: test every reference, as the reference kernel's
@@ -507,7 +497,7 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, Best& b, Tr
         test_ref<METRICS>(S, (int)((unsigned)ref >> kTypeShift), ref & kIndexMask, o, d, dd, b, c);
       }
     }
-  } else {
+  } else if (active) {
     for (int i = 0; i < S.count[kSphere]; ++i)
       offer(S, b, sphere_test<false>(__ldg(S.spheres + i), o, d, dd, nullptr), kSphere, i);
     for (int i = 0; i < S.count[kBox]; ++i)
@@ -531,6 +521,7 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, Best& b, Tr
       c->type[4] += S.count[3];
     }
   }
+  if (!active) return false;
   // tracePlane, K:708-734: a plane wins only when strictly closer.
   for (int i = 0; i < S.plane_count; ++i) {
     float4 p = __ldg(S.planes + i);

@@ -53,7 +53,7 @@ __device__ __forceinline__ uint32_t pixel_base_seed(unsigned long long frame_see
 }
 
 template <bool METRICS>
-__global__ void __launch_bounds__(128) k_render(RenderArgs a) {
+__global__ void __launch_bounds__(128, 8) k_render(RenderArgs a) {
   const DevScene& S = a.S;
   const int lane = threadIdx.x & 31;
   TraceCounters c{};
@@ -112,10 +112,11 @@ __global__ void __launch_bounds__(128) k_render(RenderArgs a) {
     }
     // ---- one path segment (tracePath loop body, K:1098-1162)
     bool finished = !done && !path;  // max_depth == 0: the sample is black
-    if (!done && path) {
+    bool tracing = !done && path;
+    Best b;
+    bool hit = trace_closest<METRICS>(S, o, d, tracing, b, &c, nullptr);
+    if (tracing) {
       if (METRICS) rays++;
-      Best b;
-      bool hit = trace_closest<METRICS>(S, o, d, b, &c, nullptr);
       if (!hit) {
         rad = add(rad, mulv(thr, S.background));
         finished = true;
@@ -203,13 +204,17 @@ __global__ void __launch_bounds__(256) k_trace(DevScene S, const float* rays, in
                                                float* dist, int* order, int* mat, float* normal,
                                                unsigned long long* counters) {
   int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= n) return;
-  const float* ry = rays + 6 * (size_t)r;
-  float3 o = v3(ry[0], ry[1], ry[2]);
-  float3 d = v3(ry[3], ry[4], ry[5]);
+  bool active = r < n;  // every lane stays for the warp-cooperative traversal
+  float3 o = v3(0.0f, 0.0f, 0.0f), d = v3(0.0f, 0.0f, 1.0f);
+  if (active) {
+    const float* ry = rays + 6 * (size_t)r;
+    o = v3(ry[0], ry[1], ry[2]);
+    d = v3(ry[3], ry[4], ry[5]);
+  }
   TraceCounters c{};
   Best b;
-  bool hit = trace_closest<METRICS>(S, o, d, b, &c, nullptr);
+  bool hit = trace_closest<METRICS>(S, o, d, active, b, &c, nullptr);
+  if (!active) return;
   float3 pos, nn = v3(0, 0, 0);
   int mi = -1;
   if (hit) hit_record(S, b, o, d, &pos, &nn, &mi);
