@@ -14,3 +14,4 @@ for p in (ROOT, os.path.join(ROOT, "master-rad_b200")):
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (sm_100a) and the built library")
+    config.addinivalue_line("markers", "slow: full-size (million-primitive) cases")
