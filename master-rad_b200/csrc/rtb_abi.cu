@@ -117,6 +117,13 @@ rtb_status rtb_context_create(int device, rtb_context** out) {
     delete ctx;
     return RTB_ERR_UNAVAILABLE;  // built for sm_100a only
   }
+  // Keep freed stream-ordered allocations in this process's default pool (the builder and
+  // scene arenas allocate from it on every build).
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
@@ -208,8 +215,7 @@ rtb_status rtb_scene_download_bvh(rtb_context* ctx, const rtb_scene* scene, floa
 rtb_status rtb_scene_destroy(rtb_context* ctx, rtb_scene* scene) {
   if (!ctx || !scene) return RTB_ERR_INVALID_ARGUMENT;
   Guard g(ctx);
-  cudaStreamSynchronize(ctx->stream);
-  scene_free(scene);
+  scene_free(scene, ctx->stream);
   return RTB_OK;
 }
 

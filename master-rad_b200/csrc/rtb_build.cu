@@ -475,14 +475,16 @@ __global__ void k_flatten(const Prims P, IdxSet I, const Nodes N, int count, flo
 
 inline unsigned blocks(long long n, int b = 256) { return (unsigned)std::max<long long>(1, (n + b - 1) / b); }
 
+// Build workspace from the device's stream-ordered pool: after the first build the pool
+// holds the memory, so later builds allocate without a device-wide synchronisation.
 struct Workspace {
   std::vector<void*> ptrs;
-  rtb_context* ctx;
+  cudaStream_t stream = nullptr;
   bool ok = true;
   template <typename T>
   T* alloc(size_t n) {
     void* p = nullptr;
-    if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) {
+    if (cudaMallocAsync(&p, std::max<size_t>(n, 1) * sizeof(T), stream) != cudaSuccess) {
       ok = false;
       return nullptr;
     }
@@ -490,7 +492,7 @@ struct Workspace {
     return (T*)p;
   }
   ~Workspace() {
-    for (void* p : ptrs) cudaFree(p);
+    for (void* p : ptrs) cudaFreeAsync(p, stream);
   }
 };
 
@@ -532,7 +534,7 @@ rtb_status build_bvh(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_bui
   const int n = c.total;
   cudaStream_t sm = ctx->stream;
   Workspace W;
-  W.ctx = ctx;
+  W.stream = sm;
   // ---- inputs
   float* d_sph = W.alloc<float>((size_t)c.n[0] * 5);
   float* d_box = W.alloc<float>((size_t)c.n[1] * 7);

@@ -400,22 +400,19 @@ __device__ __forceinline__ float prune_limit(float t) {
 }
 
 template <bool METRICS>
-__device__ __forceinline__ void trace_leaf(const DevScene& S, int first, int meta, float3 o, float3 d,
-                                           float dd, Best& b, TraceCounters* c) {
-  int count = meta & 0xFFFFFF;
-  int code = meta >> 24;
-  if (METRICS) {
-    c->leaf++;
-    if (code == 4)
-      c->mixed++;
-    else
-      c->homo++;
+__device__ __noinline__ void test_all_refs(const DevScene& S, float3 o, float3 d, float dd, Best& b,
+                                           TraceCounters* c) {
+  for (int i = 0; i < S.ref_count; ++i) {
+    int ref = __ldg(S.refs + i);
+    test_ref<METRICS>(S, (int)((unsigned)ref >> kTypeShift), ref & kIndexMask, o, d, dd, b, c);
   }
-  for (int i = 0; i < count; ++i) {
-    int ref = __ldg(S.refs + first + i);
-    int type = code == 4 ? (int)((unsigned)ref >> kTypeShift) : code;
-    test_ref<METRICS>(S, type, ref & kIndexMask, o, d, dd, b, c);
-  }
+}
+
+template <bool METRICS>
+__device__ __noinline__ void test_all_primitives(const DevScene& S, float3 o, float3 d, float dd,
+                                                 Best& b, TraceCounters* c) {
+  for (int t = 0; t < 4; ++t)
+    for (int i = 0; i < S.count[t]; ++i) test_ref<METRICS>(S, t, i, o, d, dd, b, c);
 }
 
 // Closest hit of one ray against the resident scene (traceClosest, K:963-1020): the BVH
@@ -423,9 +420,9 @@ __device__ __forceinline__ void trace_leaf(const DevScene& S, int first, int met
 //
 // Warp-cooperative: all 32 lanes of the warp call it together (lanes without a ray pass
 // active = false).  The traversal loop is warp-uniform -- each iteration every lane that
-// still has work processes one node (testing both child boxes and any leaf child
-// immediately) and the loop condition is a warp vote -- so divergent lanes reconverge once
-// per node instead of drifting apart for a whole traversal.
+// still has work processes one node: it tests both child boxes, then tests the primitives
+// of the (at most two) leaf children in one loop, then picks the next interior node -- and
+// the loop condition is a warp vote, so divergent lanes reconverge once per node.
 template <bool METRICS>
 __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active, Best& b,
                               TraceCounters* c, int* overflow_flag) {
@@ -443,7 +440,7 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
     int node = active ? 0 : -1;
     bool overflow = false;
     // A tree visits each node at most once per ray; the cap only matters for malformed
-    // (cyclic) caller-supplied trees, which then take the exhaustive path below.
+    // (cyclic) caller-supplied trees, which then take the exhaustive path.
     int budget = S.node_count + 8;
     while (__any_sync(0xFFFFFFFFu, node >= 0)) {
       if (node >= 0) {
@@ -461,11 +458,33 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
         float en = swap ? e1 : e0, ef = swap ? e0 : e1;
         int ln = swap ? n3.y : n3.x, lf = swap ? n3.x : n3.y;
         int mn = swap ? n3.w : n3.z, mf = swap ? n3.z : n3.w;
-        if (en != CUDART_INF_F && ln < 0) trace_leaf<METRICS>(S, ~ln, mn, o, d, dd, b, c);
-        if (ef != CUDART_INF_F && lf < 0 && ef <= prune_limit(b.t))
-          trace_leaf<METRICS>(S, ~lf, mf, o, d, dd, b, c);
-        int next = (en != CUDART_INF_F && ln >= 0) ? ln : -1;
-        if (ef != CUDART_INF_F && lf >= 0 && ef <= prune_limit(b.t)) {
+        bool hn = en != CUDART_INF_F, hf = ef != CUDART_INF_F;
+        // Leaf children: one loop over the near leaf's references then the far leaf's.
+        // Testing the far leaf even if the near one already beats it is harmless: the
+        // closest hit is a minimum over primitives.
+        int first0 = (hn && ln < 0) ? ~ln : 0, count0 = (hn && ln < 0) ? (mn & 0xFFFFFF) : 0;
+        int first1 = (hf && lf < 0) ? ~lf : 0, count1 = (hf && lf < 0) ? (mf & 0xFFFFFF) : 0;
+        int code0 = mn >> 24, code1 = mf >> 24;
+        if (METRICS) {
+          if (count0 || (hn && ln < 0)) {
+            c->leaf++;
+            if (code0 == 4) c->mixed++; else c->homo++;
+          }
+          if (count1 || (hf && lf < 0)) {
+            c->leaf++;
+            if (code1 == 4) c->mixed++; else c->homo++;
+          }
+        }
+        for (int k = 0; k < count0 + count1; ++k) {
+          bool second = k >= count0;
+          int ref = __ldg(S.refs + (second ? first1 + (k - count0) : first0 + k));
+          int code = second ? code1 : code0;
+          int type = code == 4 ? (int)((unsigned)ref >> kTypeShift) : code;
+          test_ref<METRICS>(S, type, ref & kIndexMask, o, d, dd, b, c);
+        }
+        float plim = prune_limit(b.t);
+        int next = (hn && ln >= 0) ? ln : -1;
+        if (hf && lf >= 0 && ef <= plim) {
           if (next < 0) {
             next = lf;
           } else if (sp < kStackSize) {
@@ -478,7 +497,6 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
           }
         }
         // Pop the next subtree still closer than the current hit.
-        float plim = prune_limit(b.t);
         while (next < 0 && sp > 0) {
           --sp;
           if (estack[sp] <= plim) next = stack[sp];
@@ -488,38 +506,12 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
       }
     }
     if (overflow) {
-      // A tree deeper than the stack: test every reference, as the reference kernel's
-      // overflow path does (K:942-959); the result is the same closest hit.
       if (overflow_flag) atomicAdd(overflow_flag, 1);
       if (METRICS) c->overflow++;
-      for (int i = 0; i < S.ref_count; ++i) {
-        int ref = __ldg(S.refs + i);
-        test_ref<METRICS>(S, (int)((unsigned)ref >> kTypeShift), ref & kIndexMask, o, d, dd, b, c);
-      }
+      test_all_refs<METRICS>(S, o, d, dd, b, c);
     }
   } else if (active) {
-    for (int i = 0; i < S.count[kSphere]; ++i)
-      offer(S, b, sphere_test<false>(__ldg(S.spheres + i), o, d, dd, nullptr), kSphere, i);
-    for (int i = 0; i < S.count[kBox]; ++i)
-      offer(S, b, box_test<false>(__ldg(S.boxes + 2 * i), __ldg(S.boxes + 2 * i + 1), o, d, nullptr),
-            kBox, i);
-    for (int i = 0; i < S.count[kAffineSphere]; ++i) {
-      const float4* r = S.aspheres + 3 * i;
-      offer(S, b, affine_sphere_test<false>(__ldg(r), __ldg(r + 1), __ldg(r + 2), o, d, dd, nullptr, nullptr),
-            kAffineSphere, i);
-    }
-    for (int i = 0; i < S.count[kAffineBox]; ++i) {
-      const float4* r = S.aboxes + 3 * i;
-      offer(S, b, affine_box_test<false>(__ldg(r), __ldg(r + 1), __ldg(r + 2), o, d, dd, nullptr, nullptr),
-            kAffineBox, i);
-    }
-    if (METRICS) {
-      c->prim += S.count[0] + S.count[1] + S.count[2] + S.count[3];
-      c->type[0] += S.count[0];
-      c->type[1] += S.count[1];
-      c->type[3] += S.count[2];
-      c->type[4] += S.count[3];
-    }
+    test_all_primitives<METRICS>(S, o, d, dd, b, c);
   }
   if (!active) return false;
   // tracePlane, K:708-734: a plane wins only when strictly closer.
@@ -564,7 +556,7 @@ __device__ __forceinline__ int plane_material(const float* p, float3 hp) {
 
 // The full hit record of the winner: position o + d t, the reference's normal for that
 // primitive type, and its material index.
-__device__ __forceinline__ void hit_record(const DevScene& S, const Best& b, float3 o, float3 d,
+static __device__ __noinline__ void hit_record(const DevScene& S, const Best& b, float3 o, float3 d,
                                            float3* pos, float3* n, int* material) {
   float dd = dot(d, d);
   *pos = add(o, mul(d, b.t));

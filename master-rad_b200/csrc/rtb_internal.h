@@ -59,7 +59,7 @@ rtb_status scene_create(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_
                         const float* d_node_bounds, const int* d_node_data, int node_count,
                         const int* d_refs, int ref_count, const int* d_roots, int root_count,
                         rtb_scene** out);
-void scene_free(rtb_scene* s);
+void scene_free(rtb_scene* s, cudaStream_t stream);
 
 // rtb_render.cu
 rtb_status render_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,

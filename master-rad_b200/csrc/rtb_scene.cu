@@ -259,10 +259,10 @@ inline unsigned blocks(long long n, int b = 256) { return (unsigned)((n + b - 1)
 
 }  // namespace
 
-void scene_free(rtb_scene* s) {
+void scene_free(rtb_scene* s, cudaStream_t stream) {
   if (!s) return;
-  cudaFree(s->arena);
-  for (void* p : s->extra) cudaFree(p);
+  cudaFreeAsync(s->arena, stream);
+  for (void* p : s->extra) cudaFreeAsync(p, stream);
   delete s;
 }
 
@@ -389,7 +389,7 @@ rtb_status scene_create(rtb_context* ctx, const rtb_scene_desc* d, const rtb_bvh
   size_t o_nodes = ar.take<float4>(4 * (size_t)(synth + interior));
 
   rtb_scene* s = new rtb_scene();
-  cudaError_t e = cudaMalloc(&s->arena, ar.off);
+  cudaError_t e = cudaMallocAsync(&s->arena, ar.off, sm);
   if (e != cudaSuccess) {
     delete s;
     return cuda_fail(ctx, e, "scene arena");
@@ -425,15 +425,15 @@ rtb_status scene_create(rtb_context* ctx, const rtb_scene_desc* d, const rtb_bvh
     cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, sm);
     e = cudaStreamSynchronize(sm);
     if (e != cudaSuccess) {
-      scene_free(s);
+      scene_free(s, sm);
       return cuda_fail(ctx, e, "BVH reference check");
     }
     if (herr & 1) {
-      scene_free(s);
+      scene_free(s, sm);
       return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "BVH reference index out of range");
     }
     if (herr & (4 | 8)) {
-      scene_free(s);
+      scene_free(s, sm);
       return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "BVH node child or leaf range out of range");
     }
     // A permutation needs every primitive referenced exactly once (no duplicates).
@@ -487,15 +487,15 @@ rtb_status scene_create(rtb_context* ctx, const rtb_scene_desc* d, const rtb_bvh
   e = cudaStreamSynchronize(sm);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) {
-    scene_free(s);
+    scene_free(s, sm);
     return cuda_fail(ctx, e, "scene packing");
   }
   if (herr & (1 | 4 | 8)) {
-    scene_free(s);
+    scene_free(s, sm);
     return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "BVH arrays failed the device range checks");
   }
   if (herr & 16) {
-    scene_free(s);
+    scene_free(s, sm);
     return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "material index outside the material table");
   }
 
