@@ -172,6 +172,22 @@ RTB_API rtb_status rtb_render_device(rtb_context* ctx, rtb_scene* scene, const r
 /* GpuRayTracer.lastFrameStats / lastPhysicalKernelLaunchCount (GpuRayTracer.java:294-306). */
 RTB_API rtb_status rtb_last_frame_stats(rtb_context* ctx, rtb_frame_stats* out);
 
+/* Closest-hit replay that allocates nothing.  No counterpart in the reference.
+ * For callers that cannot allocate device memory when they query (a host framework that
+ * owns a fixed device-memory budget, a frame loop that forbids allocation after start-up):
+ * same results as rtb_trace_replay on a resident scene, but rays and hit records are staged
+ * in a fixed array of RTB_STATIC_REPLAY_MAX_RAYS rays inside the library, and the call makes
+ * no cudaMalloc/cudaFree or other allocation.  Every GPU that loads the library holds that
+ * array (about 3.4 MB) until exit.  The first call on a device looks up the array's address
+ * (so make it before any stream capture).  Calls share the array: calls that overlap on the
+ * GPU race.  Returns RTB_ERR_LIMIT for ray_count > RTB_STATIC_REPLAY_MAX_RAYS.  Runs on the
+ * scene's device on the calling thread's per-thread default stream and returns when the
+ * host outputs are written. */
+#define RTB_STATIC_REPLAY_MAX_RAYS 65536
+RTB_API rtb_status rtb_trace_replay_static(const rtb_scene* scene, const float* rays, int ray_count,
+                                           int use_bvh, int* hit_flags, float* hit_distances,
+                                           int* hit_orders, int* hit_materials, float* hit_normals);
+
 /* Host-writable abort: running persistent kernels of this context stop at their next
  * work fetch and the call returns RTB_ERR_WATCHDOG.  Cleared by the next render call. */
 RTB_API rtb_status rtb_request_abort(rtb_context* ctx);

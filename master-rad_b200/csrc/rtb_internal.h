@@ -41,6 +41,7 @@ struct rtb_scene {
   int* ref_roots = nullptr;
   int ref_node_count = 0, ref_ref_count = 0, ref_root_count = 0;
   bool has_bvh = false;
+  int device = 0;  // the device the scene is resident on
   std::vector<void*> extra;  // additional allocations freed with the scene
 };
 
@@ -65,6 +66,9 @@ void scene_free(rtb_scene* s, cudaStream_t stream);
 rtb_status render_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
                         const rtb_render_params* p, float* d_rgb, cudaStream_t stream,
                         bool timed);
+// Closest-hit launch without a context (no counters, no allocation).
+cudaError_t launch_trace(const DevScene& scene, int use_bvh, const float* d_rays, int n, int* d_flags,
+                         float* d_t, int* d_order, int* d_mat, float* d_normal, cudaStream_t stream);
 rtb_status trace_rays(rtb_context* ctx, rtb_scene* scene, const float* d_rays, int n, int use_bvh,
                       int collect_metrics, int* d_flags, float* d_t, int* d_order, int* d_mat,
                       float* d_normal, cudaStream_t stream);

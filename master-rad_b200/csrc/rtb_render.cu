@@ -295,6 +295,16 @@ rtb_status render_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* ca
   return RTB_OK;
 }
 
+cudaError_t launch_trace(const DevScene& scene, int use_bvh, const float* d_rays, int n, int* d_flags,
+                         float* d_t, int* d_order, int* d_mat, float* d_normal, cudaStream_t stream) {
+  DevScene S = scene;
+  S.use_bvh = use_bvh ? scene.use_bvh : 0;
+  if (n > 0)
+    k_trace<false><<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(S, d_rays, n, d_flags, d_t, d_order,
+                                                                    d_mat, d_normal, nullptr);
+  return cudaGetLastError();
+}
+
 rtb_status trace_rays(rtb_context* ctx, rtb_scene* scene, const float* d_rays, int n, int use_bvh,
                       int collect_metrics, int* d_flags, float* d_t, int* d_order, int* d_mat,
                       float* d_normal, cudaStream_t stream) {

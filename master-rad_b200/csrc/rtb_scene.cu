@@ -525,6 +525,7 @@ rtb_status scene_create(rtb_context* ctx, const rtb_scene_desc* d, const rtb_bvh
   D.background = make_float3(d->background[0], d->background[1], d->background[2]);
   D.use_bvh = has_bvh ? 1 : 0;
   s->has_bvh = has_bvh;
+  s->device = ctx->device;
   s->ref_node_bounds = (float*)(A + o_rnb);
   s->ref_node_data = (int*)(A + o_rnd);
   s->ref_refs = (int*)(A + o_rrf);

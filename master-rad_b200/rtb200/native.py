@@ -98,7 +98,10 @@ SIGNATURES = {
                                     C.POINTER(RenderParams), C.c_void_p, C.c_void_p]),
     "rtb_last_frame_stats": (C.c_int, [C.c_void_p, C.POINTER(FrameStats)]),
     "rtb_request_abort": (C.c_int, [C.c_void_p]),
+    "rtb_trace_replay_static": (C.c_int, [C.c_void_p, FP, C.c_int, C.c_int, IP, FP, IP, IP, FP]),
 }
+
+STATIC_REPLAY_MAX_RAYS = 65536  # RTB_STATIC_REPLAY_MAX_RAYS in include/rtb200.h
 
 _lib = None
 

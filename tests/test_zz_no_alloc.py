@@ -1,0 +1,77 @@
+"""rtb_trace_replay_static: the closest-hit replay that allocates nothing.
+
+Callers that cannot allocate device memory when they query (a host framework owning a fixed
+device-memory budget, a frame loop that forbids allocation after start-up) use this entry
+point; it stages rays and hits in the library's fixed device array instead of a cudaMalloc'd
+buffer.  Its results must equal rtb_trace_replay's bit for bit (the tolerance the other
+closest-hit parity tests use), on two calls in a row, since the array keeps the previous
+call's contents.  This file sorts last so that a run stopping at the first failure has run
+every other test first; it also passes alone in a fresh process.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from rtb200 import native as N
+from rtb200 import synth
+from rtb200.tracer import Context, ResidentScene
+
+pytestmark = pytest.mark.gpu
+
+
+def _replay(ctx, rs, rays, static):
+    n = len(rays)
+    r = N.f32(rays).reshape(-1)
+    out = dict(hit=np.full(n, -7, np.int32), t=np.full(n, np.nan, np.float32),
+               order=np.full(n, -7, np.int32), material=np.full(n, -7, np.int32),
+               normal=np.full(3 * n, np.nan, np.float32))
+    args = (N.iptr(out["hit"]), N.fptr(out["t"]), N.iptr(out["order"]), N.iptr(out["material"]),
+            N.fptr(out["normal"]))
+    if static:
+        st = ctx.lib.rtb_trace_replay_static(rs.handle, N.fptr(r), n, 1, *args)
+        assert st == N.RTB_OK, N.STATUS_NAMES.get(st, st)
+    else:
+        ctx.check(ctx.lib.rtb_trace_replay(ctx.handle, rs.handle, N.fptr(r), n, 1, 0, *args))
+    return out
+
+
+def _same(a, b):
+    for k in ("hit", "order", "material"):
+        np.testing.assert_array_equal(a[k], b[k])
+    np.testing.assert_array_equal(a["t"].view(np.int32), b["t"].view(np.int32))
+    np.testing.assert_array_equal(a["normal"].view(np.int32), b["normal"].view(np.int32))
+
+
+def test_static_replay_matches_allocating_replay_twice():
+    ctx = Context(0)
+    try:
+        scene = synth.hetero_scene(3000, 31, synth.WORKLOAD_IDS["test"], 12)
+        rs = ResidentScene.build(ctx, scene)
+        cam = synth.camera_looking_z((0.0, 0.0, -2.9))
+        first = np.concatenate([synth.primary_grid(cam, 96, 64), synth.random_rays(5000, 41)])
+        second = synth.random_rays(2000, 43)  # fewer rays: stale slots must not leak through
+        for rays in (first, second):
+            _same(_replay(ctx, rs, rays, True), _replay(ctx, rs, rays, False))
+        assert _replay(ctx, rs, first, True)["hit"].sum() > 0
+        rs.close()
+    finally:
+        ctx.close()
+
+
+def test_static_replay_rejects_more_rays_than_its_array():
+    ctx = Context(0)
+    try:
+        scene = synth.hetero_scene(200, 5, synth.WORKLOAD_IDS["test"], 13)
+        rs = ResidentScene.build(ctx, scene)
+        n = N.STATIC_REPLAY_MAX_RAYS + 1
+        rays = np.zeros(6 * n, np.float32)
+        outs = [np.zeros(n, np.int32), np.zeros(n, np.float32), np.zeros(n, np.int32),
+                np.zeros(n, np.int32), np.zeros(3 * n, np.float32)]
+        st = ctx.lib.rtb_trace_replay_static(rs.handle, N.fptr(rays), n, 1, N.iptr(outs[0]),
+                                             N.fptr(outs[1]), N.iptr(outs[2]), N.iptr(outs[3]),
+                                             N.fptr(outs[4]))
+        assert st == 8  # RTB_ERR_LIMIT
+        rs.close()
+    finally:
+        ctx.close()
