@@ -172,6 +172,37 @@ RTB_API rtb_status rtb_render_device(rtb_context* ctx, rtb_scene* scene, const r
 /* GpuRayTracer.lastFrameStats / lastPhysicalKernelLaunchCount (GpuRayTracer.java:294-306). */
 RTB_API rtb_status rtb_last_frame_stats(rtb_context* ctx, rtb_frame_stats* out);
 
+/* ---- batched rendering (no counterpart in the reference, which renders one scene per
+ *      renderSample call) ----
+ * A batch renders many resident scenes -- each with its own camera, resolution, sample count
+ * and depth -- in one persistent launch over a shared pixel queue, captured once into a CUDA
+ * graph and replayed by rtb_batch_render.  Every job's image equals its rtb_render_device
+ * frame bit for bit.  Output buffers are caller-owned device arrays (3 floats per pixel). */
+typedef struct {
+  rtb_scene* scene;
+  rtb_camera camera;
+  rtb_render_params params;   /* use_bvh is honoured; collect_metrics is ignored */
+  float* rgb_device;
+} rtb_batch_job;
+
+typedef struct {
+  int threads_per_block;      /* 64, 128 or 256 */
+  int job_order;              /* 0: as given, 1: most expensive jobs first */
+} rtb_batch_tuning;
+
+typedef struct rtb_batch rtb_batch;
+
+/* tuning may be NULL (128 threads, most expensive first). */
+RTB_API rtb_status rtb_batch_create(rtb_context* ctx, const rtb_batch_job* jobs, int job_count,
+                                    const rtb_batch_tuning* tuning, rtb_batch** out);
+/* Replays the batch's graph on `stream` (NULL: the context stream); returns once queued. */
+RTB_API rtb_status rtb_batch_render(rtb_context* ctx, rtb_batch* batch, void* stream);
+/* Times every candidate tuning on the batch itself (`repeats` timed runs each after a
+ * warm-up run), keeps the fastest, re-captures the graph and reports it. */
+RTB_API rtb_status rtb_batch_autotune(rtb_context* ctx, rtb_batch* batch, int repeats,
+                                      rtb_batch_tuning* best, double* best_ms);
+RTB_API rtb_status rtb_batch_destroy(rtb_context* ctx, rtb_batch* batch);
+
 /* Closest-hit replay that allocates nothing.  No counterpart in the reference.
  * For callers that cannot allocate device memory when they query (a host framework that
  * owns a fixed device-memory budget, a frame loop that forbids allocation after start-up):

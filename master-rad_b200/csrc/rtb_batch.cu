@@ -1,0 +1,404 @@
+// Batched rendering: many resident scenes, each with its own camera, resolution, sample count
+// and depth, rendered by ONE persistent launch over a shared pixel queue and replayed from a
+// captured CUDA graph.
+//
+// The per-scene form launches one frame per scene; small frames (256x256 = 65,536 pixels)
+// cannot fill 148 SMs and every launch ends in its own tail.  Here the pixels of all jobs form
+// one index space: a lane that finishes a pixel takes the next index of the batch queue, which
+// may belong to another scene, so the GPU stays full until the whole batch's last pixels.
+// Each pixel still runs its samples in order with the reference's random streams and FP32
+// running sum (GpuKernelSources.java:1231-1293, tracePath K:1061-1165), so every job's image
+// is bit-identical to its per-scene frame.
+//
+// Launch parameters (threads per block, job order) come from rtb_batch_autotune, which times
+// the candidates on the batch itself.
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "rtb_internal.h"
+
+struct rtb_batch {
+  std::vector<rtb_batch_job> jobs;  // in the caller's order
+  void* d_jobs = nullptr;           // device job table (in the tuned order)
+  long long total_pixels = 0;
+  rtb_batch_tuning tuning{};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int device = 0;
+};
+
+namespace rtb {
+namespace {
+
+constexpr int kMaxSharedJobs = 256;
+
+struct BatchJob {
+  DevScene S;
+  float3 cam_pos, cam_f, cam_r, cam_u;
+  int width, height, spp, max_depth, frame_index;
+  unsigned long long frame_seed;
+  float* out;
+  long long begin;  // first batch pixel index of this job
+};
+
+__device__ __forceinline__ float luminance(float3 c) {  // K:181-183
+  return c.x * 0.212655f + c.y * 0.715158f + c.z * 0.072187f;
+}
+__device__ __forceinline__ float3 reflect_dir(float3 n, float3 i) {  // K:1022-1024
+  return sub(mul(n, 2.0f * dot(i, n)), i);
+}
+__device__ __forceinline__ float3 refract_dir(float3 incoming, float3 n, float eta) {  // K:1026-1039
+  float3 i = normalize_safe(incoming);
+  float c1 = dot(i, n);
+  float ri = (c1 >= 0.0f) ? eta : -1.0f / eta;
+  float inv_ri2 = 1.0f / (ri * ri);
+  float c2 = 1.0f - (1.0f - c1 * c1) * inv_ri2;
+  if (c2 <= 0.0f) return normalize_safe(reflect_dir(n, i));
+  float sq = sqrtf(c2);
+  return normalize_safe(sub(mul(n, c1 - sq * ri), i));
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_batch(const BatchJob* jobs, int njobs,
+                                                                   long long total,
+                                                                   unsigned long long* queue,
+                                                                   const int* abort_flag) {
+  __shared__ long long s_begin[kMaxSharedJobs];
+  const int nshared = njobs < kMaxSharedJobs ? njobs : kMaxSharedJobs;
+  for (int j = threadIdx.x; j < nshared; j += THREADS) s_begin[j] = jobs[j].begin;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  int job = 0;
+  long long pixel = -1;
+  int x = 0, y = 0, so = 0;
+  uint32_t base_seed = 0, rng = 0;
+  float3 acc = v3(0, 0, 0), thr = v3(0, 0, 0), rad = v3(0, 0, 0), o = v3(0, 0, 0), d = v3(0, 0, 0);
+  int depth = 0;
+  bool path = false, done = false;
+  while (true) {
+    // ---- fetch a batch pixel (warp-aggregated) and find its job
+    bool need = !done && pixel < 0;
+    unsigned need_mask = __ballot_sync(0xFFFFFFFFu, need);
+    if (need_mask) {
+      unsigned long long basep = 0;
+      int leader = __ffs(need_mask) - 1;
+      if (lane == leader)
+        basep = (*(volatile const int*)abort_flag) ? (unsigned long long)total
+                                                   : atomicAdd(queue, (unsigned long long)__popc(need_mask));
+      basep = __shfl_sync(0xFFFFFFFFu, basep, leader);
+      if (need) {
+        long long g = (long long)basep + __popc(need_mask & ((1u << lane) - 1u));
+        if (g >= total) {
+          done = true;
+        } else {
+          int lo = 0, hi = njobs - 1;  // last job with begin <= g
+          while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            long long b = mid < kMaxSharedJobs ? s_begin[mid] : jobs[mid].begin;
+            if (b <= g) lo = mid; else hi = mid - 1;
+          }
+          job = lo;
+          const BatchJob& J = jobs[job];
+          pixel = g - J.begin;
+          x = (int)(pixel % J.width);
+          y = (int)(pixel / J.width);
+          so = 0;
+          uint32_t s = hash_u32((uint32_t)(J.frame_seed & 0xFFFFFFFFULL));  // K:1231-1236
+          s ^= hash_u32((uint32_t)(J.frame_seed >> 32));
+          s ^= hash_u32((uint32_t)J.frame_index);
+          s ^= hash_u32((uint32_t)y * (uint32_t)J.width + (uint32_t)x);
+          base_seed = hash_u32(s);
+        }
+      }
+    }
+    if (__all_sync(0xFFFFFFFFu, done)) break;
+    const BatchJob& J = jobs[job];
+    // ---- start a sample (K:1251-1264)
+    if (!done && !path) {
+      uint32_t seed = base_seed ^ hash_u32((uint32_t)so);
+      seed ^= hash_u32((uint32_t)(so * 0x9E3779B9u));
+      rng = hash_u32(seed);
+      float jx = rand01(&rng) - 0.5f;
+      float jy = rand01(&rng) - 0.5f;
+      float aspect = (float)J.width / (float)J.height;
+      float u = ((((float)x + 0.5f) + jx) * (2.0f / (float)J.width) - 1.0f) * aspect;
+      float v = 1.0f - ((((float)y + 0.5f) + jy) * (2.0f / (float)J.height));
+      o = J.cam_pos;
+      d = add(add(J.cam_f, mul(J.cam_r, u)), mul(J.cam_u, v));
+      thr = v3(1.0f, 1.0f, 1.0f);
+      rad = v3(0.0f, 0.0f, 0.0f);
+      depth = 0;
+      path = J.max_depth > 0;
+    }
+    // ---- one path segment (K:1098-1162)
+    bool finished = !done && !path;
+    bool tracing = !done && path;
+    Best b;
+    bool hit = trace_closest<false>(J.S, o, d, tracing, b, nullptr, nullptr);
+    if (tracing) {
+      if (!hit) {
+        rad = add(rad, mulv(thr, J.S.background));
+        finished = true;
+      } else {
+        float3 pos, n;
+        int mi;
+        hit_record(J.S, b, o, d, &pos, &n, &mi);
+        float4 m0 = make_float4(0, 0, 0, 0), m1 = m0, m2 = m0, m3 = m0;
+        if (mi >= 0) {
+          const float4* mp = J.S.materials + 4 * mi;
+          m0 = __ldg(mp);
+          m1 = __ldg(mp + 1);
+          m2 = __ldg(mp + 2);
+          m3 = __ldg(mp + 3);
+        }
+        float3 cd = v3(m0.x, m0.y, m0.z), cr = v3(m1.x, m1.y, m1.z), ct = v3(m2.x, m2.y, m2.z);
+        rad = add(rad, mulv(thr, v3(m3.x, m3.y, m3.z)));
+        float3 inc = neg(d);
+        float wd = luminance(cd), wr = luminance(cr), wt = luminance(ct);
+        float sum = wd + wr + wt;
+        if (sum <= 0.0f) {
+          finished = true;
+        } else {
+          float xi = rand01(&rng) * sum;
+          float3 nd, wc;
+          if (xi < wd) {
+            float pc = wd / sum;
+            float z = rand01(&rng) * 2.0f - 1.0f;
+            float t = rand01(&rng) * 2.0f * CUDART_PI_F;
+            float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+            nd = add(v3(r * cosf(t), r * sinf(t), z), n);
+            wc = divs(cd, pc);
+          } else if (xi < wd + wr) {
+            float pc = wr / sum;
+            nd = reflect_dir(n, inc);
+            wc = divs(cr, pc);
+          } else {
+            float pc = wt / sum;
+            nd = refract_dir(inc, n, m0.w);
+            wc = divs(ct, pc);
+          }
+          o = add(pos, mul(nd, kEps));
+          thr = mulv(thr, wc);
+          d = nd;
+          depth++;
+          if (depth >= J.max_depth) finished = true;
+        }
+      }
+    }
+    if (finished) {
+      path = false;
+      acc = so == 0 ? rad : add(acc, rad);
+      so++;
+      if (so == J.spp) {
+        acc = mul(acc, 1.0f / (float)J.spp);
+        float* out = J.out + 3 * pixel;
+        out[0] = acc.x;
+        out[1] = acc.y;
+        out[2] = acc.z;
+        pixel = -1;
+      }
+    }
+  }
+}
+
+int launch_grid(rtb_context* ctx, int threads, long long total) {
+  int bps = 1;
+  const void* fn = threads == 64 ? (const void*)k_batch<64>
+                 : threads == 256 ? (const void*)k_batch<256> : (const void*)k_batch<128>;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, threads, 0);
+  if (bps < 1) bps = 1;
+  long long want = (total + threads - 1) / threads;
+  return (int)std::max<long long>(1, std::min<long long>((long long)ctx->sm_count * bps, want));
+}
+
+rtb_status enqueue(rtb_context* ctx, rtb_batch* B, cudaStream_t sm) {
+  int threads = B->tuning.threads_per_block;
+  int grid = launch_grid(ctx, threads, B->total_pixels);
+  cudaMemsetAsync(ctx->d_work, 0, sizeof(unsigned long long), sm);
+  const BatchJob* J = (const BatchJob*)B->d_jobs;
+  int n = (int)B->jobs.size();
+  if (threads == 64)
+    k_batch<64><<<grid, 64, 0, sm>>>(J, n, B->total_pixels, ctx->d_work, ctx->d_abort);
+  else if (threads == 256)
+    k_batch<256><<<grid, 256, 0, sm>>>(J, n, B->total_pixels, ctx->d_work, ctx->d_abort);
+  else
+    k_batch<128><<<grid, 128, 0, sm>>>(J, n, B->total_pixels, ctx->d_work, ctx->d_abort);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? RTB_OK : cuda_fail(ctx, e, "batch launch");
+}
+
+// Job table in the tuned order: order 0 keeps the caller's order, order 1 puts the most
+// expensive jobs (pixels x spp x depth) first so the batch does not end on a large frame.
+rtb_status upload_jobs(rtb_context* ctx, rtb_batch* B) {
+  std::vector<int> order(B->jobs.size());
+  std::iota(order.begin(), order.end(), 0);
+  if (B->tuning.job_order == 1) {
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+      const rtb_render_params& pa = B->jobs[a].params;
+      const rtb_render_params& pb = B->jobs[b].params;
+      double ca = (double)pa.width * pa.height * pa.samples_per_frame * std::max(1, pa.max_depth);
+      double cb = (double)pb.width * pb.height * pb.samples_per_frame * std::max(1, pb.max_depth);
+      return ca > cb;
+    });
+  }
+  std::vector<BatchJob> h(order.size());
+  long long begin = 0;
+  for (size_t k = 0; k < order.size(); ++k) {
+    const rtb_batch_job& j = B->jobs[order[k]];
+    BatchJob& b = h[k];
+    b.S = j.scene->dev;
+    b.S.use_bvh = (j.params.use_bvh && j.scene->has_bvh) ? 1 : 0;
+    b.cam_pos = make_float3(j.camera.position[0], j.camera.position[1], j.camera.position[2]);
+    b.cam_f = make_float3(j.camera.forward[0], j.camera.forward[1], j.camera.forward[2]);
+    b.cam_r = make_float3(j.camera.right[0], j.camera.right[1], j.camera.right[2]);
+    b.cam_u = make_float3(j.camera.up[0], j.camera.up[1], j.camera.up[2]);
+    b.width = j.params.width;
+    b.height = j.params.height;
+    b.spp = j.params.samples_per_frame;
+    b.max_depth = j.params.max_depth;
+    b.frame_index = j.params.frame_index;
+    b.frame_seed = j.params.frame_seed;
+    b.out = j.rgb_device;
+    b.begin = begin;
+    begin += (long long)j.params.width * j.params.height;
+  }
+  if (!B->d_jobs) {
+    cudaError_t e = cudaMalloc(&B->d_jobs, sizeof(BatchJob) * h.size());
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "batch job table");
+  }
+  cudaError_t e = cudaMemcpy(B->d_jobs, h.data(), sizeof(BatchJob) * h.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "batch job table upload");
+  B->total_pixels = begin;
+  return RTB_OK;
+}
+
+rtb_status capture(rtb_context* ctx, rtb_batch* B) {
+  if (B->exec) cudaGraphExecDestroy(B->exec);
+  if (B->graph) cudaGraphDestroy(B->graph);
+  B->exec = nullptr;
+  B->graph = nullptr;
+  cudaStream_t sm = ctx->stream;
+  cudaError_t e = cudaStreamBeginCapture(sm, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "batch graph capture");
+  rtb_status s = enqueue(ctx, B, sm);
+  e = cudaStreamEndCapture(sm, &B->graph);
+  if (s != RTB_OK) return s;
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "batch graph capture");
+  e = cudaGraphInstantiate(&B->exec, B->graph, 0);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "batch graph instantiate");
+  return RTB_OK;
+}
+
+}  // namespace
+}  // namespace rtb
+
+using namespace rtb;
+
+extern "C" {
+
+rtb_status rtb_batch_create(rtb_context* ctx, const rtb_batch_job* jobs, int job_count,
+                            const rtb_batch_tuning* tuning, rtb_batch** out) {
+  if (!ctx) return RTB_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  cudaSetDevice(ctx->device);
+  if (!jobs || job_count < 1 || !out) return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "a batch needs jobs");
+  for (int k = 0; k < job_count; ++k) {
+    const rtb_batch_job& j = jobs[k];
+    const rtb_render_params& p = j.params;
+    if (!j.scene || !j.rgb_device || p.width < 1 || p.height < 1 || p.samples_per_frame < 1 ||
+        p.max_depth < 0 || p.max_depth > 32)
+      return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "invalid batch job " + std::to_string(k));
+    if (j.scene->device != ctx->device)
+      return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "batch job scene is on another device");
+  }
+  rtb_batch* B = new rtb_batch();
+  B->device = ctx->device;
+  B->jobs.assign(jobs, jobs + job_count);
+  B->tuning.threads_per_block = 128;
+  B->tuning.job_order = 1;
+  if (tuning) B->tuning = *tuning;
+  if (B->tuning.threads_per_block != 64 && B->tuning.threads_per_block != 128 &&
+      B->tuning.threads_per_block != 256) {
+    delete B;
+    return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "threads_per_block must be 64, 128 or 256");
+  }
+  rtb_status s = upload_jobs(ctx, B);
+  if (s == RTB_OK) s = capture(ctx, B);
+  if (s != RTB_OK) {
+    cudaFree(B->d_jobs);
+    delete B;
+    return s;
+  }
+  *out = B;
+  return RTB_OK;
+}
+
+rtb_status rtb_batch_render(rtb_context* ctx, rtb_batch* B, void* stream) {
+  if (!ctx || !B) return RTB_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  cudaSetDevice(ctx->device);
+  cudaStream_t sm = stream ? (cudaStream_t)stream : ctx->stream;
+  cudaMemsetAsync(ctx->d_abort, 0, sizeof(int), sm);
+  cudaError_t e = cudaGraphLaunch(B->exec, sm);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "batch graph launch");
+  return RTB_OK;
+}
+
+rtb_status rtb_batch_autotune(rtb_context* ctx, rtb_batch* B, int repeats, rtb_batch_tuning* best,
+                              double* best_ms) {
+  if (!ctx || !B) return RTB_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  cudaSetDevice(ctx->device);
+  if (repeats < 1) repeats = 1;
+  const int threads[3] = {64, 128, 256};
+  double best_time = 1e300;
+  rtb_batch_tuning pick = B->tuning;
+  cudaStream_t sm = ctx->stream;
+  for (int order = 0; order < 2; ++order) {
+    for (int t : threads) {
+      B->tuning.threads_per_block = t;
+      B->tuning.job_order = order;
+      rtb_status s = upload_jobs(ctx, B);
+      if (s != RTB_OK) return s;
+      double total = 0.0;
+      for (int r = 0; r <= repeats; ++r) {  // first run warms up
+        cudaEventRecord(ctx->ev0, sm);
+        s = enqueue(ctx, B, sm);
+        if (s != RTB_OK) return s;
+        cudaEventRecord(ctx->ev1, sm);
+        cudaError_t e = cudaEventSynchronize(ctx->ev1);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "batch autotune");
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        if (r > 0) total += ms;
+      }
+      double mean = total / repeats;
+      if (mean < best_time) {
+        best_time = mean;
+        pick = B->tuning;
+      }
+    }
+  }
+  B->tuning = pick;
+  rtb_status s = upload_jobs(ctx, B);
+  if (s == RTB_OK) s = capture(ctx, B);
+  if (s != RTB_OK) return s;
+  if (best) *best = pick;
+  if (best_ms) *best_ms = best_time;
+  return RTB_OK;
+}
+
+rtb_status rtb_batch_destroy(rtb_context* ctx, rtb_batch* B) {
+  if (!ctx || !B) return RTB_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  if (B->exec) cudaGraphExecDestroy(B->exec);
+  if (B->graph) cudaGraphDestroy(B->graph);
+  cudaFree(B->d_jobs);
+  delete B;
+  return RTB_OK;
+}
+
+}  // extern "C"

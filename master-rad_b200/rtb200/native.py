@@ -76,6 +76,15 @@ class FrameStats(C.Structure):
                 ("physical_launches", C.c_int)]
 
 
+class BatchJob(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("camera", Camera), ("params", RenderParams),
+                ("rgb_device", C.c_void_p)]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("threads_per_block", C.c_int), ("job_order", C.c_int)]
+
+
 # Every symbol include/rtb200.h declares, with its ctypes signature.
 SIGNATURES = {
     "rtb_context_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
@@ -99,6 +108,12 @@ SIGNATURES = {
     "rtb_last_frame_stats": (C.c_int, [C.c_void_p, C.POINTER(FrameStats)]),
     "rtb_request_abort": (C.c_int, [C.c_void_p]),
     "rtb_trace_replay_static": (C.c_int, [C.c_void_p, FP, C.c_int, C.c_int, IP, FP, IP, IP, FP]),
+    "rtb_batch_create": (C.c_int, [C.c_void_p, C.POINTER(BatchJob), C.c_int, C.POINTER(BatchTuning),
+                                   C.POINTER(C.c_void_p)]),
+    "rtb_batch_render": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "rtb_batch_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(BatchTuning),
+                                     C.POINTER(C.c_double)]),
+    "rtb_batch_destroy": (C.c_int, [C.c_void_p, C.c_void_p]),
 }
 
 STATIC_REPLAY_MAX_RAYS = 65536  # RTB_STATIC_REPLAY_MAX_RAYS in include/rtb200.h
