@@ -184,37 +184,46 @@ __global__ void k_gather_weights(const Prims P, const int* idx, int n, double* w
   if (j < n) wpos[j] = P.w[idx[j]];
 }
 
-// Sequential prefix / suffix construction weights of one (node, direction) in axis order.
-// wpos holds the weights in axis order, so the dependent-add chain streams contiguous memory.
-__global__ void k_weights(const double* wpos, const Nodes N, const int* active, int k,
-                          int weighted, double* pw, double* sw) {
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= 2 * k) return;
-  int node = active[g >> 1];
+// Unit construction weights: prefix / suffix sums are exact integers, one thread per position.
+__global__ void k_weights_unit(const Nodes N, const int* key, const int* level_of, int level, int n,
+                               double* pw, double* sw) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  int node = key[j];
+  if (level_of[node] != level) return;
+  int s = N.start[node], e = N.end[node];
+  pw[j] = (double)(j - s + 1);
+  sw[j] = (double)(e - j);
+}
+
+// Weighted prefix / suffix sums in the reference's sequential order, one warp per
+// (node, direction): the warp loads 32 weights at a time (coalesced) and every lane runs the
+// same strictly sequential add chain over the shuffled values, lane j keeping the running
+// sum after element j.  The additions happen in exactly the Java loop's order, so every
+// partial sum is bit-identical to it; only the loads are parallel.
+__global__ void k_weights_seq(const double* wpos, const Nodes N, const int* active, int k, double* pw,
+                              double* sw) {
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (warp >= 2 * k) return;
+  int node = active[warp >> 1];
   int s = N.start[node], e = N.end[node];
   if (e - s < 2) return;
-  if (!weighted) {
-    if (g & 1) {
-      for (int j = e - 1; j >= s; --j) sw[j] = (double)(e - j);
-    } else {
-      for (int j = s; j < e; ++j) pw[j] = (double)(j - s + 1);
+  bool suffix = warp & 1;
+  int n = e - s;
+  double acc = 0.0;
+  for (int base = 0; base < n; base += 32) {
+    int j = base + lane;
+    int pos = suffix ? e - 1 - j : s + j;
+    double w = j < n ? wpos[pos] : 0.0;
+    int m = min(32, n - base);
+    double mine = 0.0;
+    for (int q = 0; q < m; ++q) {
+      double v = __shfl_sync(0xFFFFFFFFu, w, q);
+      acc = (base == 0 && q == 0) ? v : acc + v;
+      if (q == lane) mine = acc;
     }
-    return;
-  }
-  if (g & 1) {
-    double acc = wpos[e - 1];
-    sw[e - 1] = acc;
-    for (int j = e - 2; j >= s; --j) {
-      acc = acc + wpos[j];
-      sw[j] = acc;
-    }
-  } else {
-    double acc = wpos[s];
-    pw[s] = acc;
-    for (int j = s + 1; j < e; ++j) {
-      acc = acc + wpos[j];
-      pw[j] = acc;
-    }
+    if (j < n) (suffix ? sw : pw)[pos] = mine;
   }
 }
 
@@ -675,8 +684,12 @@ rtb_status build_bvh(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_bui
       tb = tmp_bytes;
       cub::DeviceScan::InclusiveScanByKey(tmp, tb, key_rev, boxes, suf, BoxUnion(), n,
                                           cub::Equality(), sm);
-      if (c.weighted) k_gather_weights<<<blocks(n), 256, 0, sm>>>(P, I.a[a], n, wpos);
-      k_weights<<<blocks(2LL * k, 128), 128, 0, sm>>>(wpos, N, active, k, c.weighted, pw, sw);
+      if (c.weighted) {
+        k_gather_weights<<<blocks(n), 256, 0, sm>>>(P, I.a[a], n, wpos);
+        k_weights_seq<<<blocks(64LL * k, 128), 128, 0, sm>>>(wpos, N, active, k, pw, sw);
+      } else {
+        k_weights_unit<<<blocks(n), 256, 0, sm>>>(N, key, level_of, level, n, pw, sw);
+      }
       k_costs<<<blocks(n), 256, 0, sm>>>(P, I.a[a], N, key, level_of, level, a, n,
                                          a == 0 ? pre0 : pre, suf, pw, sw, c.traversal, cost[a]);
     }
