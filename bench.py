@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="hetero", choices=["hetero", "plain", "scale", "batched"])
+    ap.add_argument("--workload", default="hetero", choices=["hetero", "plain", "scale", "batched", "adjoint"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     # size overrides for small profiling captures of the same scene
@@ -272,6 +272,110 @@ def run_batched(args):
     ctx.close()
 
 
+def pick_parameters(g, n_albedo, count, rng):
+    """Random parameters for the finite-difference check: half albedo, half emission, from
+    those whose gradient is at least 1e-2 (else 1e-3, 1e-4) of the largest in their group --
+    smaller gradients are below the finite difference's FP32 image noise."""
+    out = []
+    for lo, hi in ((0, n_albedo), (n_albedo, len(g))):
+        grp = np.abs(g[lo:hi])
+        if grp.size == 0 or grp.max() == 0:
+            continue
+        for frac in (1e-2, 1e-3, 1e-4):
+            cand = np.nonzero(grp >= frac * grp.max())[0]
+            if len(cand) >= count // 2:
+                break
+        take = min(count // 2, len(cand))
+        out.extend((lo + rng.choice(cand, size=take, replace=False)).tolist())
+    return np.array(out, dtype=np.int64)
+
+
+def run_adjoint(args):
+    """The differentiable workload: 4096-primitive mixed scene, 512x512, 32 spp, depth 6; L2
+    image loss against a target rendered with albedos perturbed by N(0, 0.05) (12-uniform
+    approximation, clamped to [0, 1]); forward frame vs path-replay backward time, and the
+    relative error against central finite differences (h = 1e-3, common random numbers, FP64
+    loss) on 64 random parameters whose gradient is at least 1 % of the largest."""
+    import torch
+    from rtb200.diff import DifferentiableScene
+    torch.cuda.set_device(0)
+    ctx = Context(0)
+    w = synth.adjoint_workload()
+    ds = DifferentiableScene(ctx, w.scene, w.width, w.height, w.spp, w.max_depth, w.camera,
+                             w.frame_index, w.frame_seed)
+    alb0, emi0 = ds.albedo(), ds.emission()
+    st = synth.Stream(1, synth.WORKLOAD_IDS["adjoint"], 1, 7)
+    u12 = st.uniform(12 * alb0.size).reshape(-1, 3, 12)
+    g12 = u12[:, :, 0].copy()
+    for j in range(1, 12):
+        g12 = g12 + u12[:, :, j]
+    target_alb = np.clip(alb0 + 0.05 * (g12 - 6.0) * (alb0 > 0), 0.0, 1.0)
+    n = w.width * w.height * 3
+    img = torch.empty(n, dtype=torch.float32, device="cuda")
+    ga = torch.empty(ds.count * 3, dtype=torch.float32, device="cuda")
+    ge = torch.empty(ds.count * 3, dtype=torch.float32, device="cuda")
+    sobj = torch.cuda.Stream()
+    stream = sobj.cuda_stream
+
+    def render(alb, emi):
+        ds.set_parameters(alb, emi)
+        ds.render_into(img.data_ptr(), stream)
+        sobj.synchronize()
+        return img.cpu().numpy().astype(np.float64)
+
+    target = render(target_alb, emi0)
+    base = render(alb0, emi0)
+    adj = torch.from_numpy((2.0 * (base - target)).astype(np.float32)).cuda()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fwd, bwd = [], []
+    torch.cuda.synchronize()
+    for i in range(args.warmup + args.steps):
+        e0.record(sobj)
+        ds.render_into(img.data_ptr(), stream)
+        e1.record(sobj)
+        e1.synchronize()
+        if i >= args.warmup:
+            fwd.append(e0.elapsed_time(e1))
+        e0.record(sobj)
+        ds.backward_into(adj.data_ptr(), ga.data_ptr(), ge.data_ptr(), stream)
+        e1.record(sobj)
+        e1.synchronize()
+        if i >= args.warmup:
+            bwd.append(e0.elapsed_time(e1))
+    sobj.synchronize()
+    g = np.concatenate([ga.cpu().numpy(), ge.cpu().numpy()]).astype(np.float64)
+    pick = pick_parameters(g, ga.numel(), 64, np.random.default_rng(1))
+    h = 1e-3
+    errs = []
+    for idx in pick:
+        alb, emi = alb0.copy(), emi0.copy()
+        arr, k = (alb, idx) if idx < alb.size else (emi, idx - alb.size)
+        flat = arr.reshape(-1)
+        v = flat[k]
+        flat[k] = v + h
+        lp = float(np.sum((render(alb, emi) - target) ** 2))
+        flat[k] = v - h
+        lm = float(np.sum((render(alb, emi) - target) ** 2))
+        fd = (lp - lm) / (2 * h)
+        errs.append(abs(g[idx] - fd) / max(abs(fd), 1e-12))
+    errs = np.array(errs)
+    samples = w.width * w.height * w.spp
+    f_ms, b_ms = statistics.mean(fwd), statistics.mean(bwd)
+    line = {"metric": "Msamples/s", "value": samples / (b_ms / 1e3) / 1e6, "unit": "Msamples/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": b_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "adjoint-4k 512x512 32spp depth6", "materials": ds.count,
+                       "parameters": 6 * ds.count},
+            "forward_ms": f_ms, "backward_ms": b_ms, "backward_over_forward": b_ms / f_ms,
+            "fd_check": {"parameters": int(len(errs)), "h": h, "max_rel_err": float(errs.max()),
+                         "median_rel_err": float(np.median(errs))},
+            "gpu_launches": args.steps}
+    print(json.dumps(line), flush=True)
+    ds.close()
+    ctx.close()
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -282,6 +386,9 @@ def main():
         return
     if args.workload == "batched":
         run_batched(args)
+        return
+    if args.workload == "adjoint":
+        run_adjoint(args)
         return
     import torch
     import torch.distributed as dist

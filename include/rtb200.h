@@ -172,6 +172,21 @@ RTB_API rtb_status rtb_render_device(rtb_context* ctx, rtb_scene* scene, const r
 /* GpuRayTracer.lastFrameStats / lastPhysicalKernelLaunchCount (GpuRayTracer.java:294-306). */
 RTB_API rtb_status rtb_last_frame_stats(rtb_context* ctx, rtb_frame_stats* out);
 
+/* ---- differentiable rendering (no counterpart in the reference) ----
+ * rtb_scene_set_materials replaces a resident scene's 13-float material records (same
+ * count), e.g. with perturbed or optimised albedos and emissions; the next frames use them.
+ * rtb_render_backward is the adjoint of rtb_render_device for the same scene, camera and
+ * params: given dLoss/dImage (device, 3 floats per pixel) it re-traces every sample from its
+ * random seed and writes dLoss/d(albedo) and dLoss/d(emission) per material record (device,
+ * 3 floats per material each; zeroed first).  Albedo is the diffuse colour; the lobe choice
+ * is not differentiated (exact for diffuse-only materials). */
+RTB_API rtb_status rtb_scene_set_materials(rtb_context* ctx, rtb_scene* scene, const float* materials,
+                                           int material_count);
+RTB_API rtb_status rtb_render_backward(rtb_context* ctx, rtb_scene* scene, const rtb_camera* camera,
+                                       const rtb_render_params* params, const float* adjoint_device,
+                                       float* grad_albedo_device, float* grad_emission_device,
+                                       void* stream);
+
 /* ---- batched rendering (no counterpart in the reference, which renders one scene per
  *      renderSample call) ----
  * A batch renders many resident scenes -- each with its own camera, resolution, sample count

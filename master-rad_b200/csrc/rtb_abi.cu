@@ -127,6 +127,7 @@ rtb_status rtb_context_create(int device, rtb_context** out) {
   e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->order_ev, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_work, 32 * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_abort, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(ctx->d_abort, 0, sizeof(int));
@@ -150,6 +151,7 @@ rtb_status rtb_context_destroy(rtb_context* ctx) {
     cudaFreeHost(ctx->h_pinned);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->order_ev) cudaEventDestroy(ctx->order_ev);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
   }
   delete ctx;
@@ -171,7 +173,9 @@ rtb_status rtb_scene_upload(rtb_context* ctx, const rtb_scene_desc* desc, const 
   if (!ctx) return RTB_ERR_INVALID_ARGUMENT;
   Guard g(ctx);
   auto t0 = Clock::now();
+  ctx_acquire(ctx, ctx->stream);
   rtb_status s = scene_create(ctx, desc, bvh, nullptr, nullptr, 0, nullptr, 0, nullptr, 0, out);
+  ctx_release(ctx, ctx->stream);
   if (s == RTB_OK) ctx->last.upload_ns = ns_since(t0);
   return s;
 }
@@ -181,7 +185,9 @@ rtb_status rtb_scene_build(rtb_context* ctx, const rtb_scene_desc* desc, const r
   if (!ctx) return RTB_ERR_INVALID_ARGUMENT;
   Guard g(ctx);
   auto t0 = Clock::now();
+  ctx_acquire(ctx, ctx->stream);
   rtb_status s = build_bvh(ctx, desc, config, out, stats);
+  ctx_release(ctx, ctx->stream);
   if (s == RTB_OK) ctx->last.upload_ns = ns_since(t0);
   return s;
 }
@@ -215,7 +221,9 @@ rtb_status rtb_scene_download_bvh(rtb_context* ctx, const rtb_scene* scene, floa
 rtb_status rtb_scene_destroy(rtb_context* ctx, rtb_scene* scene) {
   if (!ctx || !scene) return RTB_ERR_INVALID_ARGUMENT;
   Guard g(ctx);
+  ctx_acquire(ctx, ctx->stream);
   scene_free(scene, ctx->stream);
+  ctx_release(ctx, ctx->stream);
   return RTB_OK;
 }
 
@@ -245,6 +253,7 @@ rtb_status rtb_trace_replay(rtb_context* ctx, rtb_scene* scene, const float* ray
   o += al(n * 4);
   float* d_n = (float*)(sb + o);
   cudaStream_t sm = ctx->stream;
+  ctx_acquire(ctx, sm);
   cudaMemcpyAsync(d_rays, rays, n * 24, cudaMemcpyHostToDevice, sm);
   cudaEventRecord(ctx->ev0, sm);
   rtb_status s = trace_rays(ctx, scene, d_rays, ray_count, use_bvh, collect_metrics, d_f, d_t, d_o, d_m, d_n, sm);
@@ -255,6 +264,7 @@ rtb_status rtb_trace_replay(rtb_context* ctx, rtb_scene* scene, const float* ray
   cudaMemcpyAsync(hit_orders, d_o, n * 4, cudaMemcpyDeviceToHost, sm);
   cudaMemcpyAsync(hit_materials, d_m, n * 4, cudaMemcpyDeviceToHost, sm);
   cudaMemcpyAsync(hit_normals, d_n, n * 12, cudaMemcpyDeviceToHost, sm);
+  ctx_release(ctx, sm);
   cudaError_t e = cudaStreamSynchronize(sm);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "trace replay");
   float ms = 0.0f;
@@ -276,8 +286,11 @@ rtb_status rtb_render_device(rtb_context* ctx, rtb_scene* scene, const rtb_camer
   if (!ctx) return RTB_ERR_INVALID_ARGUMENT;
   Guard g(ctx);
   cudaStream_t sm = stream ? (cudaStream_t)stream : ctx->stream;
+  ctx_acquire(ctx, sm);
   cudaMemsetAsync(ctx->d_abort, 0, sizeof(int), sm);
-  return render_frame(ctx, scene, camera, params, rgb_device, sm, false);
+  rtb_status s = render_frame(ctx, scene, camera, params, rgb_device, sm, false);
+  ctx_release(ctx, sm);
+  return s;
 }
 
 rtb_status rtb_render_sample(rtb_context* ctx, rtb_scene* scene, const rtb_camera* camera,
@@ -290,8 +303,10 @@ rtb_status rtb_render_sample(rtb_context* ctx, rtb_scene* scene, const rtb_camer
   float* d_rgb = (float*)stage(ctx, bytes);
   if (!d_rgb) return fail(ctx, RTB_ERR_OUT_OF_MEMORY, "output staging");
   cudaStream_t sm = ctx->stream;
+  ctx_acquire(ctx, sm);
   cudaMemsetAsync(ctx->d_abort, 0, sizeof(int), sm);
   rtb_status s = render_frame(ctx, scene, camera, params, d_rgb, sm, true);
+  ctx_release(ctx, sm);
   if (s != RTB_OK) return s;
   cudaError_t e = cudaEventSynchronize(ctx->ev1);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "render");

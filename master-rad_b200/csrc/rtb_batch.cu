@@ -339,8 +339,10 @@ rtb_status rtb_batch_render(rtb_context* ctx, rtb_batch* B, void* stream) {
   std::lock_guard<std::mutex> lock(ctx->mu);
   cudaSetDevice(ctx->device);
   cudaStream_t sm = stream ? (cudaStream_t)stream : ctx->stream;
+  ctx_acquire(ctx, sm);
   cudaMemsetAsync(ctx->d_abort, 0, sizeof(int), sm);
   cudaError_t e = cudaGraphLaunch(B->exec, sm);
+  ctx_release(ctx, sm);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "batch graph launch");
   return RTB_OK;
 }
@@ -355,6 +357,7 @@ rtb_status rtb_batch_autotune(rtb_context* ctx, rtb_batch* B, int repeats, rtb_b
   double best_time = 1e300;
   rtb_batch_tuning pick = B->tuning;
   cudaStream_t sm = ctx->stream;
+  ctx_acquire(ctx, sm);
   for (int order = 0; order < 2; ++order) {
     for (int t : threads) {
       B->tuning.threads_per_block = t;
@@ -381,6 +384,7 @@ rtb_status rtb_batch_autotune(rtb_context* ctx, rtb_batch* B, int repeats, rtb_b
     }
   }
   B->tuning = pick;
+  ctx_release(ctx, sm);
   rtb_status s = upload_jobs(ctx, B);
   if (s == RTB_OK) s = capture(ctx, B);
   if (s != RTB_OK) return s;

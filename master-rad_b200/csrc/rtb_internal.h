@@ -16,6 +16,11 @@ struct rtb_context {
   char name[256] = {0};
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // Orders all device work of the context across streams: the work queue, counters and
+  // staging buffers below are shared, so a launch on one stream must not overlap the
+  // context's previous launch on another.
+  cudaEvent_t order_ev = nullptr;
+  bool order_pending = false;
   std::mutex mu;
   std::string last_error;
   rtb_frame_stats last{};
@@ -46,6 +51,16 @@ struct rtb_scene {
 };
 
 namespace rtb {
+
+// Makes `s` wait for the context's previous device work, and marks `s` as holding the
+// latest.  Every entry point that enqueues work brackets it with these.
+inline void ctx_acquire(rtb_context* ctx, cudaStream_t s) {
+  if (ctx->order_pending) cudaStreamWaitEvent(s, ctx->order_ev, 0);
+}
+inline void ctx_release(rtb_context* ctx, cudaStream_t s) {
+  cudaEventRecord(ctx->order_ev, s);
+  ctx->order_pending = true;
+}
 
 // Status helpers.
 rtb_status fail(rtb_context* ctx, rtb_status s, const std::string& msg);

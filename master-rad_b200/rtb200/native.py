@@ -114,6 +114,10 @@ SIGNATURES = {
     "rtb_batch_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(BatchTuning),
                                      C.POINTER(C.c_double)]),
     "rtb_batch_destroy": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "rtb_scene_set_materials": (C.c_int, [C.c_void_p, C.c_void_p, FP, C.c_int]),
+    "rtb_render_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Camera),
+                                      C.POINTER(RenderParams), C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p]),
 }
 
 STATIC_REPLAY_MAX_RAYS = 65536  # RTB_STATIC_REPLAY_MAX_RAYS in include/rtb200.h

@@ -38,6 +38,7 @@ def lib():
         _lib.orc_trace.restype = None
         _lib.orc_render.restype = None
         _lib.orc_cpu_render.restype = C.c_int
+        _lib.orc_adjoint.restype = None
     return _lib
 
 
@@ -242,3 +243,24 @@ def cpu_render(workload, frames=None, rows=None, threads=0, seed=0x68EFD508E309A
                          _fp(_f32(w.scene.background)), _ip(params), C.c_ulonglong(seed),
                          r0, r1, threads, out.ctypes.data_as(C.POINTER(C.c_double)))
     return out.reshape(-1, 3)
+
+
+def adjoint(workload, adjoint_image, bvh=None, use_bvh=True, materials=None):
+    """FP64 restatement of the path-replay adjoint (orc_adjoint): dLoss/d(albedo) and
+    dLoss/d(emission) per material for dLoss/dI = adjoint_image (H*W*3)."""
+    w = workload
+    sa = _SceneArgs(w.scene, bvh, use_bvh)
+    if materials is not None:
+        sa.arrs[5] = _f32(materials).reshape(-1)
+        sa.ptrs[5] = _fp(sa.arrs[5])
+    cam = _f32(w.camera.packed())
+    bg = _f32(w.scene.background)
+    adj = _f32(adjoint_image).reshape(-1)
+    m = int(sa.counts[5])
+    ga = np.zeros(3 * m, np.float64)
+    ge = np.zeros(3 * m, np.float64)
+    lib().orc_adjoint(*sa.args(), _fp(cam), _fp(bg), _ip(_render_params(w)),
+                      C.c_ulonglong(w.frame_seed), 0, w.width * w.height, _fp(adj),
+                      ga.ctypes.data_as(C.POINTER(C.c_double)),
+                      ge.ctypes.data_as(C.POINTER(C.c_double)))
+    return ga.reshape(-1, 3), ge.reshape(-1, 3)

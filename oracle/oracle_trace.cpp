@@ -818,4 +818,117 @@ void orc_render(const float* const* arrays, const int* counts, const int* bvh_in
   }
 }
 
+// FP64 adjoint of the sample loop for a pixel range (test infrastructure): the FP32 path of
+// orc_render, with dLoss/d(albedo) and dLoss/d(emission) per material accumulated in double
+// along the path backward (Li <- E + W Li), the lobe probability held fixed.  adjoint holds
+// dLoss/dI (3 floats per pixel of the whole image); grads are 3 doubles per material each.
+void orc_adjoint(const float* const* arrays, const int* counts, const int* bvh_ints,
+                 const float* node_bounds, const int* node_data, const int* refs, const int* roots,
+                 const float* camera, const float* background, const int* params,
+                 unsigned long long frame_seed, int pixel_begin, int pixel_end, const float* adjoint,
+                 double* grad_albedo, double* grad_emission) {
+  Scene s = make_scene(arrays, counts, bvh_ints, node_bounds, node_data, refs, roots);
+  int width = params[0], height = params[1], spp = params[2], max_depth = params[3];
+  int frame_index = params[4];
+  f3 cp = mk(camera[0], camera[1], camera[2]);
+  f3 cf = mk(camera[3], camera[4], camera[5]);
+  f3 cr = mk(camera[6], camera[7], camera[8]);
+  f3 cu = mk(camera[9], camera[10], camera[11]);
+  f3 bg = mk(background[0], background[1], background[2]);
+  const float* M = s.materials;
+  for (int p = pixel_begin; p < pixel_end; ++p) {
+    int x = p % width, y = p / width;
+    uint32_t base = hash_u32((uint32_t)(frame_seed & 0xFFFFFFFFULL));
+    base ^= hash_u32((uint32_t)(frame_seed >> 32));
+    base ^= hash_u32((uint32_t)frame_index);
+    base ^= hash_u32((uint32_t)y * (uint32_t)width + (uint32_t)x);
+    base = hash_u32(base);
+    double adj[3] = {adjoint[3 * p] / (double)spp, adjoint[3 * p + 1] / (double)spp,
+                     adjoint[3 * p + 2] / (double)spp};
+    for (int so = 0; so < spp; ++so) {
+      uint32_t seed = base ^ hash_u32((uint32_t)so);
+      seed ^= hash_u32((uint32_t)so * 0x9E3779B9u);
+      seed = hash_u32(seed);
+      uint32_t rng = seed;
+      float jx = rand01(&rng) - 0.5f;
+      float jy = rand01(&rng) - 0.5f;
+      float aspect = (float)width / (float)height;
+      float u = ((((float)x + 0.5f) + jx) * (2.0f / (float)width) - 1.0f) * aspect;
+      float v = 1.0f - ((((float)y + 0.5f) + jy) * (2.0f / (float)height));
+      f3 o = cp, d = (cf + cr * u) + cu * v;
+      f3 thr = mk(1, 1, 1);
+      int vm[33];
+      f3 vthr[33], vw[33];
+      double vinvp[33];
+      int nv = 0;
+      bool escaped = false;
+      for (int depth = 0; depth < max_depth; ++depth) {
+        Hit h;
+        if (!trace_closest(s, o, d, &h, nullptr)) {
+          escaped = true;
+          break;
+        }
+        const float* m = h.material >= 0 ? M + 13 * h.material : nullptr;
+        f3 cd = m ? mk(m[0], m[1], m[2]) : mk(0, 0, 0);
+        f3 crf = m ? mk(m[3], m[4], m[5]) : mk(0, 0, 0);
+        f3 ct = m ? mk(m[6], m[7], m[8]) : mk(0, 0, 0);
+        float ior = m ? m[12] : 0.0f;
+        vm[nv] = h.material;
+        vthr[nv] = thr;
+        vw[nv] = mk(0, 0, 0);
+        vinvp[nv] = 0.0;
+        f3 n = h.normal, inc = -d;
+        float wd = luminance(cd), wr = luminance(crf), wt = luminance(ct);
+        float sum = (wd + wr) + wt;
+        if (sum <= 0.0f) {
+          nv++;
+          break;
+        }
+        float xi = rand01(&rng) * sum;
+        f3 nd, wc;
+        if (xi < wd) {
+          float pc = wd / sum;
+          float z = rand01(&rng) * 2.0f - 1.0f;
+          float tt = rand01(&rng) * 2.0f * 3.14159265358979323846f;
+          float r = std::sqrt(std::fmax(0.0f, 1.0f - z * z));
+          nd = mk(r * std::cos(tt), r * std::sin(tt), z) + n;
+          wc = cd / pc;
+          vinvp[nv] = 1.0 / (double)pc;
+        } else if (xi < wd + wr) {
+          float pc = wr / sum;
+          nd = reflect_dir(n, inc);
+          wc = crf / pc;
+        } else {
+          float pc = wt / sum;
+          refract_dir(inc, n, ior, &nd);
+          wc = ct / pc;
+        }
+        vw[nv] = wc;
+        nv++;
+        o = h.pos + nd * EPS;
+        thr = thr * wc;
+        d = nd;
+      }
+      double li[3] = {escaped ? (double)bg.x : 0.0, escaped ? (double)bg.y : 0.0,
+                      escaped ? (double)bg.z : 0.0};
+      for (int k = nv - 1; k >= 0; --k) {
+        int mi = vm[k];
+        double e[3] = {0, 0, 0};
+        double t3[3] = {vthr[k].x, vthr[k].y, vthr[k].z};
+        double w3[3] = {vw[k].x, vw[k].y, vw[k].z};
+        if (mi >= 0) {
+          const float* m = M + 13 * mi;
+          for (int c = 0; c < 3; ++c) {
+            e[c] = m[9 + c];
+            double basev = adj[c] * t3[c];
+            grad_emission[3 * mi + c] += basev;
+            grad_albedo[3 * mi + c] += basev * li[c] * vinvp[k];
+          }
+        }
+        for (int c = 0; c < 3; ++c) li[c] = e[c] + w3[c] * li[c];
+      }
+    }
+  }
+}
+
 }  // extern "C"
