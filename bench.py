@@ -58,7 +58,7 @@ FALLBACK_HBM_GBS = 6650.0
 TRAFFIC_BYTES_PER_SAMPLE = (12.07e6 + 42.11e6) / 2097152
 
 
-def parse():
+def parse_args(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -71,7 +71,7 @@ def parse():
     ap.add_argument("--width", type=int, default=0)
     ap.add_argument("--height", type=int, default=0)
     ap.add_argument("--spp", type=int, default=0)
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 def make_workload(name, args=None):
@@ -165,6 +165,32 @@ def cpu_baseline(w, rows, threads=0):
     dt = time.perf_counter() - t0
     samples = rows * w.width * w.spp
     return samples / dt / 1e6, dt, samples
+
+
+# Ranks render disjoint frame ranges of the same workload: rank r's frames start at
+# r * FRAMES_PER_RANK (timed frames at 0, warm-up at 1000, end-to-end at 500, counters at 0).
+FRAMES_PER_RANK = 100000
+
+
+def frame_index(rank, step, offset=0):
+    """Frame index of a rank's step; the render seeds every pixel sample from it."""
+    return rank * FRAMES_PER_RANK + offset + step
+
+
+def max_over_ranks(x, device="cuda"):
+    """Max of a scalar over the process group (the identity without one)."""
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, steps, samples_per_frame, seconds):
+    """Msamples/s of the whole job: every rank's frames over the slowest rank's time."""
+    return world * steps * samples_per_frame / seconds / 1e6
 
 
 def peak_hbm():
@@ -377,7 +403,7 @@ def run_adjoint(args):
 
 
 def main():
-    args = parse()
+    args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -423,7 +449,7 @@ def main():
     # ---- counters for the roofline: the kernel's metrics build on this rank's first frame
     #      (untimed; a host-buffer render fills rtb_frame_stats with the counters)
     host_img = np.zeros(pixels * 3, np.float32)
-    p = params(rank * 100000, 1)
+    p = params(frame_index(rank, 0), 1)
     ctx.check(lib.rtb_render_sample(ctx.handle, res.handle, C.byref(cam), C.byref(p),
                                     N.fptr(host_img)))
     fs = N.FrameStats()
@@ -436,7 +462,7 @@ def main():
     # ---- warm-up
     for i in range(args.warmup):
         with torch.cuda.stream(stream):
-            render(rank * 100000 + 1000 + i)
+            render(frame_index(rank, i, 1000))
     stream.synchronize()
 
     # ---- timed region: K frames, events around each render launch, L2 flushed between
@@ -451,7 +477,7 @@ def main():
         with torch.cuda.stream(stream):
             flush.zero_()
             starts[i].record(stream)
-            render(rank * 100000 + i)
+            render(frame_index(rank, i))
             ends[i].record(stream)
     torch.cuda.synchronize()
     if world > 1:
@@ -459,11 +485,8 @@ def main():
     clock_info = clocks.stop()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = float(sum(step_ms))
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * args.steps * samples_per_frame / (total_ms / 1e3) / 1e6
+    total_ms = max_over_ranks(total_ms)
+    value = whole_job_rate(world, args.steps, samples_per_frame, total_ms / 1e3)
     launch_ms = statistics.mean(step_ms)
     achieved = bytes_per_frame / (launch_ms / 1e3) / 1e9
     peak, peak_kind = peak_hbm()
@@ -488,18 +511,15 @@ def main():
         h = C.c_void_p()
         st = N.BvhStats()
         ctx.check(lib.rtb_scene_build(ctx.handle, C.byref(d), C.byref(bc), C.byref(h), C.byref(st)))
-        p = params(rank * 100000 + 500 + i)
+        p = params(frame_index(rank, i, 500))
         ctx.check(lib.rtb_render_sample(ctx.handle, h, C.byref(cam), C.byref(p),
                                         C.cast(C.c_void_p(img.data_ptr()), N.FP)))
         lib.rtb_scene_destroy(ctx.handle, h)
         if i >= args.warmup:
             e2e_times.append(time.perf_counter() - t0)
     e2e_total = sum(e2e_times) if e2e_times else float("nan")
-    if world > 1:
-        t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = world * args.steps * samples_per_frame / e2e_total / 1e6
+    e2e_total = max_over_ranks(e2e_total)
+    e2e_value = whole_job_rate(world, args.steps, samples_per_frame, e2e_total)
 
     line = None
     if rank == 0:
