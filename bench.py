@@ -53,9 +53,10 @@ from rtb200.tracer import Context, ResidentScene, build_config, camera_struct, s
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
-# dram__bytes_read.sum + dram__bytes_write.sum of k_render from one ncu capture of the same
-# scene at 512x512x8 spp (profiles/k_render_hetero10k_512x512x8spp_full.md), per sample.
-TRAFFIC_BYTES_PER_SAMPLE = (12.07e6 + 42.11e6) / 2097152
+# dram__bytes_read.sum + dram__bytes_write.sum of k_render per sample, from one ncu capture
+# of the same scene at 512x512x8 spp (profiles/k_render_hetero10k_512x512x8spp_full.md);
+# workloads without a capture report null traffic.
+TRAFFIC_BYTES_PER_SAMPLE = {"hetero": (12.07e6 + 42.11e6) / 2097152}
 
 
 def parse_args(argv=None):
@@ -550,9 +551,12 @@ def main():
                                 "+ image read-back, per step"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
-                         "traffic": TRAFFIC_BYTES_PER_SAMPLE * samples_per_frame,
-                         "traffic_note": "ncu capture of a 512x512x8spp frame of the same scene, "
-                                         "scaled by samples",
+                         "traffic": (TRAFFIC_BYTES_PER_SAMPLE[args.workload] * samples_per_frame
+                                     if args.workload in TRAFFIC_BYTES_PER_SAMPLE else None),
+                         "traffic_note": ("ncu capture of a 512x512x8spp frame of the same "
+                                          "scene, scaled by samples"
+                                          if args.workload in TRAFFIC_BYTES_PER_SAMPLE
+                                          else "no capture of this workload"),
                          "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
                          "algorithmic_bytes_per_launch": bytes_per_frame,
                          "launch_ms": launch_ms,

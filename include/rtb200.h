@@ -140,6 +140,15 @@ RTB_API rtb_status rtb_scene_upload(rtb_context* ctx, const rtb_scene_desc* desc
                             rtb_scene** out);
 RTB_API rtb_status rtb_scene_build(rtb_context* ctx, const rtb_scene_desc* desc,
                            const rtb_build_config* config, rtb_scene** out, rtb_bvh_stats* stats);
+/* Binned object SAH on the device: 2..32 centroid bins per axis, the configuration's
+ * per-type weights, counts accumulated by warp-aggregated atomics, FP64 split selection
+ * from integer bin counts.  No counterpart in the reference (its builder is the full sweep
+ * that rtb_scene_build reproduces node for node); the tree is deterministic and identical
+ * to this library's CPU restatement of the binned rule, not to the Java builder's.
+ * Other bin counts return RTB_ERR_INVALID_ARGUMENT. */
+RTB_API rtb_status rtb_scene_build_binned(rtb_context* ctx, const rtb_scene_desc* desc,
+                                  const rtb_build_config* config, int bins, rtb_scene** out,
+                                  rtb_bvh_stats* stats);
 /* Copies the scene's BVH back in the reference's flattened layout (for topology hashes).
  * Sizes come from rtb_scene_bvh_sizes. */
 RTB_API rtb_status rtb_scene_bvh_sizes(rtb_context* ctx, const rtb_scene* scene, int* node_count,

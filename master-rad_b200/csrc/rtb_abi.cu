@@ -192,6 +192,19 @@ rtb_status rtb_scene_build(rtb_context* ctx, const rtb_scene_desc* desc, const r
   return s;
 }
 
+rtb_status rtb_scene_build_binned(rtb_context* ctx, const rtb_scene_desc* desc,
+                                  const rtb_build_config* config, int bins, rtb_scene** out,
+                                  rtb_bvh_stats* stats) {
+  if (!ctx) return RTB_ERR_INVALID_ARGUMENT;
+  Guard g(ctx);
+  auto t0 = Clock::now();
+  ctx_acquire(ctx, ctx->stream);
+  rtb_status s = build_bvh_binned(ctx, desc, config, bins, out, stats);
+  ctx_release(ctx, ctx->stream);
+  if (s == RTB_OK) ctx->last.upload_ns = ns_since(t0);
+  return s;
+}
+
 rtb_status rtb_scene_bvh_sizes(rtb_context* ctx, const rtb_scene* scene, int* node_count,
                                int* ref_count, int* root_count) {
   if (!ctx || !scene) return RTB_ERR_INVALID_ARGUMENT;

@@ -21,115 +21,10 @@
 //    node's current order)) uses the parent's split-axis order, which is the order the
 //    Java primitives array holds when build() reaches the node.
 // The file is compiled with -fmad=false: no double expression is contracted.
-#include <cub/cub.cuh>
-
-#include <algorithm>
-#include <vector>
-
-#include "rtb_internal.h"
+#include "rtb_build_common.cuh"
 
 namespace rtb {
 namespace {
-
-struct Box {
-  float mn[3], mx[3];
-};
-
-struct BoxUnion {
-  __device__ __forceinline__ Box operator()(const Box& a, const Box& b) const {
-    Box r;
-    for (int k = 0; k < 3; ++k) {
-      r.mn[k] = fminf(a.mn[k], b.mn[k]);
-      r.mx[k] = fmaxf(a.mx[k], b.mx[k]);
-    }
-    return r;
-  }
-};
-
-// Aabb.surfaceArea (GpuScene.java:70-74) on float-valued bounds, in double.
-__device__ __forceinline__ double surface_area(const Box& b) {
-  double dx = (double)b.mx[0] - (double)b.mn[0];
-  double dy = (double)b.mx[1] - (double)b.mn[1];
-  double dz = (double)b.mx[2] - (double)b.mn[2];
-  double s = dx * dy + dx * dz;
-  s = s + dy * dz;
-  return 2.0 * s;
-}
-
-__device__ __forceinline__ float down2(float v) {
-  return nextafterf(nextafterf(v, -CUDART_INF_F), -CUDART_INF_F);
-}
-__device__ __forceinline__ float up2(float v) {
-  return nextafterf(nextafterf(v, CUDART_INF_F), CUDART_INF_F);
-}
-
-// Double.compare order as an unsigned key (-0.0 before +0.0, finite values in order).
-__device__ __forceinline__ unsigned long long order_key(double v) {
-  unsigned long long b = (unsigned long long)__double_as_longlong(v);
-  return (b >> 63) ? ~b : (b | 0x8000000000000000ULL);
-}
-
-struct Prims {
-  float* lo[3];
-  float* hi[3];
-  double* cen[3];
-  double* w;         // construction weight q = 1 + lambda (c - 1), or 1
-  double* measured;  // c
-  int* ref;
-  int* type;
-};
-
-struct BuildCfg {
-  int n[4];
-  int total;
-  int leaf_size;
-  int weighted;
-  double traversal, lambda;
-  double measured[4];
-};
-
-// Primitive bounds (GpuScene.java:626-649, 877-903) and weights.
-__global__ void k_prims(const float* spheres, const float* boxes, const float* ab, const float* bb,
-                        BuildCfg c, Prims P) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= c.total) return;
-  int t = 0, i = p;
-  while (t < 3 && i >= c.n[t]) {
-    i -= c.n[t];
-    ++t;
-  }
-  float lo[3], hi[3];
-  if (t == 0) {
-    const float* s = spheres + 5 * (size_t)i;
-    float r = s[3];
-    for (int k = 0; k < 3; ++k) {
-      lo[k] = down2(s[k] - r);
-      hi[k] = up2(s[k] + r);
-    }
-  } else if (t == 1) {
-    const float* b = boxes + 7 * (size_t)i;
-    for (int k = 0; k < 3; ++k) {
-      lo[k] = down2(b[k]);
-      hi[k] = up2(b[3 + k]);
-    }
-  } else {
-    const float* b = (t == 2 ? ab : bb) + 6 * (size_t)i;
-    for (int k = 0; k < 3; ++k) {
-      lo[k] = down2(b[k]);
-      hi[k] = up2(b[3 + k]);
-    }
-  }
-  for (int k = 0; k < 3; ++k) {
-    P.lo[k][p] = lo[k];
-    P.hi[k][p] = hi[k];
-    P.cen[k][p] = ((double)lo[k] + (double)hi[k]) * 0.5;
-  }
-  double m = c.measured[t];
-  P.measured[p] = m;
-  P.w[p] = c.weighted ? 1.0 + c.lambda * (m - 1.0) : 1.0;
-  P.ref[p] = (int)((unsigned)t << kTypeShift) | i;
-  P.type[p] = t;
-}
 
 __global__ void k_keys(const Prims P, int axis, int n, unsigned long long* keys, int* vals) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -143,26 +38,6 @@ __global__ void k_type_keys(const Prims P, const int* idx, int n, int* keys) {
   if (j < n) keys[j] = P.type[idx[j]];
 }
 
-struct Nodes {
-  int* start;
-  int* end;
-  int* order_axis;  // axis array holding the node's current order; -1: input order
-  int* depth;
-  int* left;
-  int* right;
-  int* leaf;        // 1 leaf, 0 interior
-  int* split_axis;  // this level's decision (-1: none)
-  int* split_pos;
-  Box* bounds;
-  int* size;
-  int* pre;
-  double* sah[3];   // generalized, uniform, weighted
-};
-
-__global__ void k_init_keys(int* key, const int* start, const int* end, int roots) {
-  int r = blockIdx.x;
-  for (int j = start[r] + threadIdx.x; j < end[r]; j += blockDim.x) key[j] = r;
-}
 
 __global__ void k_gather_boxes(const Prims P, const int* idx, int n, bool reverse, const int* key,
                                Box* out, int* out_key) {
@@ -295,14 +170,6 @@ __global__ void k_argmin(const Nodes N, const int* active, const double* cost0, 
   }
 }
 
-__device__ __forceinline__ int current_prim(const int* const* idx, int order_axis, int j) {
-  return order_axis < 0 ? j : idx[order_axis][j];
-}
-
-struct IdxSet {
-  int* a[3];
-};
-
 // Leaf-or-split decision per active node (GpuScene.java:1424-1447).
 __global__ void k_decide(const Prims P, IdxSet I, Nodes N, const int* active, int k,
                          const double* best_cost, const long long* best_flat, const Box* pre0,
@@ -367,173 +234,17 @@ __global__ void k_sides(IdxSet I, const Nodes N, const int* key, const int* leve
   side[p] = (j - N.start[node]) >= N.split_pos[node] ? 1 : 0;
 }
 
-__global__ void k_left_flags(const int* idx, const Nodes N, const int* key, const int* level_of,
-                             int level, int n, const unsigned char* side, int* flags) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  int node = key[j];
-  bool split = level_of[node] == level && N.split_axis[node] >= 0;
-  flags[j] = split ? (side[idx[j]] == 0) : 0;
-}
 
-__global__ void k_scatter(const int* idx, const Nodes N, const int* key, const int* level_of, int level,
-                          int n, const unsigned char* side, const int* lscan, int* out) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  int node = key[j];
-  int p = idx[j];
-  if (!(level_of[node] == level && N.split_axis[node] >= 0)) {
-    out[j] = p;
-    return;
-  }
-  int s = N.start[node];
-  int lrank = lscan[j] - lscan[s];
-  int dst = side[p] == 0 ? s + lrank : s + N.split_pos[node] + ((j - s) - lrank);
-  out[dst] = p;
-}
-
-__global__ void k_update_keys(const Nodes N, const int* level_of, int level, int n, int* key) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  int node = key[j];
-  if (level_of[node] != level || N.split_axis[node] < 0) return;
-  key[j] = j < N.start[node] + N.split_pos[node] ? N.left[node] : N.right[node];
-}
-
-// Bottom-up subtree sizes and SAH statistics (GpuScene.java:810-838) over one level.
-__global__ void k_bottom_up(const Prims P, IdxSet I, Nodes N, const int* nodes, int k,
-                            double traversal) {
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= k) return;
-  int node = nodes[g];
-  if (N.leaf[node]) {
-    N.size[node] = 1;
-    double c0 = 0.0, c1 = 0.0, c2 = 0.0;
-    for (int j = N.start[node]; j < N.end[node]; ++j) {
-      int p = current_prim(I.a, N.order_axis[node], j);
-      c0 = c0 + P.w[p];
-      c1 = c1 + 1.0;
-      c2 = c2 + P.measured[p];
-    }
-    N.sah[0][node] = c0;
-    N.sah[1][node] = c1;
-    N.sah[2][node] = c2;
-    return;
-  }
-  int l = N.left[node], r = N.right[node];
-  N.size[node] = 1 + N.size[l] + N.size[r];
-  double area = surface_area(N.bounds[node]);
-  double al = surface_area(N.bounds[l]), ar = surface_area(N.bounds[r]);
-  for (int m = 0; m < 3; ++m) {
-    double v;
-    if (!(area > 0.0)) {
-      v = N.sah[m][l] + N.sah[m][r];
-    } else {
-      double x = al / area * N.sah[m][l];
-      double y = ar / area * N.sah[m][r];
-      v = (traversal + x) + y;
-    }
-    N.sah[m][node] = v;
-  }
-}
-
-__global__ void k_preorder(Nodes N, const int* nodes, int k) {
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= k) return;
-  int node = nodes[g];
-  if (N.leaf[node]) return;
-  int l = N.left[node];
-  N.pre[l] = N.pre[node] + 1;
-  N.pre[N.right[node]] = N.pre[node] + 1 + N.size[l];
-}
-
-// Flattened reference layout (flattenBvh / leafKind, GpuScene.java:772-808).
-__global__ void k_flatten(const Prims P, IdxSet I, const Nodes N, int count, float* node_bounds,
-                          int* node_data, int* refs) {
-  int node = blockIdx.x * blockDim.x + threadIdx.x;
-  if (node >= count) return;
-  int at = N.pre[node];
-  Box b = N.bounds[node];
-  for (int k = 0; k < 3; ++k) {
-    node_bounds[6 * (size_t)at + k] = b.mn[k];
-    node_bounds[6 * (size_t)at + 3 + k] = b.mx[k];
-  }
-  int* d = node_data + 4 * (size_t)at;
-  if (!N.leaf[node]) {
-    d[0] = N.pre[N.left[node]];
-    d[1] = N.pre[N.right[node]];
-    d[2] = -1;
-    d[3] = 0;
-    return;
-  }
-  int s = N.start[node], e = N.end[node];
-  int t0 = -1;
-  bool mixed = false;
-  for (int j = s; j < e; ++j) {
-    int p = current_prim(I.a, N.order_axis[node], j);
-    refs[j] = P.ref[p];
-    int t = P.type[p];
-    if (t0 < 0) t0 = t;
-    else if (t != t0) mixed = true;
-  }
-  d[0] = mixed ? -1 : -2 - t0;
-  d[1] = -1;
-  d[2] = s;
-  d[3] = e - s;
-}
-
-inline unsigned blocks(long long n, int b = 256) { return (unsigned)std::max<long long>(1, (n + b - 1) / b); }
-
-// Build workspace from the device's stream-ordered pool: after the first build the pool
-// holds the memory, so later builds allocate without a device-wide synchronisation.
-struct Workspace {
-  std::vector<void*> ptrs;
-  cudaStream_t stream = nullptr;
-  bool ok = true;
-  template <typename T>
-  T* alloc(size_t n) {
-    void* p = nullptr;
-    if (cudaMallocAsync(&p, std::max<size_t>(n, 1) * sizeof(T), stream) != cudaSuccess) {
-      ok = false;
-      return nullptr;
-    }
-    ptrs.push_back(p);
-    return (T*)p;
-  }
-  ~Workspace() {
-    for (void* p : ptrs) cudaFreeAsync(p, stream);
-  }
-};
 
 }  // namespace
 
 rtb_status build_bvh(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_build_config* cfg,
                      rtb_scene** out, rtb_bvh_stats* stats) {
-  if (!desc || !cfg || !out) return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "null argument");
-  if (cfg->mode < 0 || cfg->mode > 7) return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "unknown BVH build mode");
-  if (cfg->mode > 3)
-    return fail(ctx, RTB_ERR_UNSUPPORTED, "SBVH and rotation build modes are not built on the device");
-  if (cfg->leaf_size < 1) return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "BVH leaf size must be positive.");
-  bool weighted = cfg->mode == 1 || cfg->mode == 3;
-  bool per_type = cfg->mode >= 2;
+  if (!out) return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "null argument");
   BuildCfg c;
-  c.n[0] = desc->sphere_count;
-  c.n[1] = desc->box_count;
-  c.n[2] = desc->affine_sphere_count;
-  c.n[3] = desc->affine_box_count;
-  for (int t = 0; t < 4; ++t)
-    if (c.n[t] < 0) return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "negative primitive count");
-  if ((c.n[2] > 0 && !desc->affine_sphere_bounds) || (c.n[3] > 0 && !desc->affine_box_bounds))
-    return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "affine bounds are required to build a BVH");
-  c.total = c.n[0] + c.n[1] + c.n[2] + c.n[3];
-  c.leaf_size = cfg->leaf_size;
-  c.weighted = weighted ? 1 : 0;
-  c.traversal = cfg->traversal_weight;
-  c.lambda = weighted ? cfg->lambda : 0.0;
-  c.measured[0] = cfg->sphere_weight;
-  c.measured[1] = cfg->box_weight;
-  c.measured[2] = cfg->affine_sphere_weight;
-  c.measured[3] = cfg->affine_box_weight;
+  bool per_type = false;
+  rtb_status st = build_setup(ctx, desc, cfg, c, per_type);
+  if (st != RTB_OK) return st;
   if (stats) *stats = rtb_bvh_stats{};
   if (c.total == 0) {
     rtb_status s = scene_create(ctx, desc, nullptr, nullptr, nullptr, 0, nullptr, 0, nullptr, 0, out);
@@ -544,41 +255,15 @@ rtb_status build_bvh(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_bui
   cudaStream_t sm = ctx->stream;
   Workspace W;
   W.stream = sm;
-  // ---- inputs
-  float* d_sph = W.alloc<float>((size_t)c.n[0] * 5);
-  float* d_box = W.alloc<float>((size_t)c.n[1] * 7);
-  float* d_ab = W.alloc<float>((size_t)c.n[2] * 6);
-  float* d_bb = W.alloc<float>((size_t)c.n[3] * 6);
-  Prims P;
-  for (int k = 0; k < 3; ++k) {
-    P.lo[k] = W.alloc<float>(n);
-    P.hi[k] = W.alloc<float>(n);
-    P.cen[k] = W.alloc<double>(n);
-  }
-  P.w = W.alloc<double>(n);
-  P.measured = W.alloc<double>(n);
-  P.ref = W.alloc<int>(n);
-  P.type = W.alloc<int>(n);
+  PrimInputs in = alloc_inputs(W, c);
+  Prims P = alloc_prims(W, n);
   IdxSet I, T;
   for (int k = 0; k < 3; ++k) {
     I.a[k] = W.alloc<int>(n);
     T.a[k] = W.alloc<int>(n);
   }
   int cap = 2 * n + 8;
-  Nodes N;
-  N.start = W.alloc<int>(cap);
-  N.end = W.alloc<int>(cap);
-  N.order_axis = W.alloc<int>(cap);
-  N.depth = W.alloc<int>(cap);
-  N.left = W.alloc<int>(cap);
-  N.right = W.alloc<int>(cap);
-  N.leaf = W.alloc<int>(cap);
-  N.split_axis = W.alloc<int>(cap);
-  N.split_pos = W.alloc<int>(cap);
-  N.bounds = W.alloc<Box>(cap);
-  N.size = W.alloc<int>(cap);
-  N.pre = W.alloc<int>(cap);
-  for (int m = 0; m < 3; ++m) N.sah[m] = W.alloc<double>(cap);
+  Nodes N = alloc_nodes(W, cap);
   int* level_of = W.alloc<int>(cap);
   int* key = W.alloc<int>(n);
   int* key_rev = W.alloc<int>(n);
@@ -619,11 +304,7 @@ rtb_status build_bvh(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_bui
   if (!W.ok) return fail(ctx, RTB_ERR_OUT_OF_MEMORY, "BVH build workspace");
 
   cudaEventRecord(ctx->ev0, sm);
-  if (c.n[0]) cudaMemcpyAsync(d_sph, desc->spheres, (size_t)c.n[0] * 20, cudaMemcpyHostToDevice, sm);
-  if (c.n[1]) cudaMemcpyAsync(d_box, desc->boxes, (size_t)c.n[1] * 28, cudaMemcpyHostToDevice, sm);
-  if (c.n[2]) cudaMemcpyAsync(d_ab, desc->affine_sphere_bounds, (size_t)c.n[2] * 24, cudaMemcpyHostToDevice, sm);
-  if (c.n[3]) cudaMemcpyAsync(d_bb, desc->affine_box_bounds, (size_t)c.n[3] * 24, cudaMemcpyHostToDevice, sm);
-  k_prims<<<blocks(n), 256, 0, sm>>>(d_sph, d_box, d_ab, d_bb, c, P);
+  upload_prims(desc, c, in, P, sm);
 
   // ---- axis orders: (centroid, order), then (type, centroid, order) for per-type forests
   for (int a = 0; a < 3; ++a) {
@@ -639,22 +320,8 @@ rtb_status build_bvh(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_bui
   }
 
   // ---- roots
-  int h_rs[4], h_re[4], roots = 0;
-  if (per_type) {
-    int off = 0;
-    for (int t = 0; t < 4; ++t) {
-      if (c.n[t] > 0) {
-        h_rs[roots] = off;
-        h_re[roots] = off + c.n[t];
-        roots++;
-      }
-      off += c.n[t];
-    }
-  } else {
-    h_rs[0] = 0;
-    h_re[0] = n;
-    roots = 1;
-  }
+  int h_rs[4], h_re[4];
+  int roots = root_ranges(c, per_type, h_rs, h_re);
   std::vector<int> h_init(roots);
   for (int r = 0; r < roots; ++r) h_init[r] = r;
   int h_counters[8] = {roots, 0, 0, 0x7FFFFFFF, 0, 0, 0, 0};
@@ -719,71 +386,8 @@ rtb_status build_bvh(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_bui
     k = next;
     level++;
   }
-  // ---- bottom-up sizes and SAH statistics, then preorder indices
-  for (int L = (int)level_begin.size() - 2; L >= 0; --L) {
-    int b = level_begin[L], cnt = level_begin[L + 1] - b;
-    k_bottom_up<<<blocks(cnt, 128), 128, 0, sm>>>(P, I, N, all_nodes + b, cnt, c.traversal);
-  }
-  // Tree roots in order: preorder index = sizes of the previous trees.
-  std::vector<int> h_size(roots);
-  for (int r = 0; r < roots; ++r) cudaMemcpyAsync(&h_size[r], N.size + r, 4, cudaMemcpyDeviceToHost, sm);
-  double h_sah[4][3];
-  for (int r = 0; r < roots; ++r)
-    for (int m = 0; m < 3; ++m) cudaMemcpyAsync(&h_sah[r][m], N.sah[m] + r, 8, cudaMemcpyDeviceToHost, sm);
-  cudaError_t e = cudaStreamSynchronize(sm);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "BVH sizes");
-  std::vector<int> h_pre(roots);
-  int acc = 0;
-  for (int r = 0; r < roots; ++r) {
-    h_pre[r] = acc;
-    acc += h_size[r];
-  }
-  cudaMemcpyAsync(N.pre, h_pre.data(), roots * 4, cudaMemcpyHostToDevice, sm);
-  for (int L = 0; L + 1 < (int)level_begin.size(); ++L) {
-    int b = level_begin[L], cnt = level_begin[L + 1] - b;
-    k_preorder<<<blocks(cnt, 128), 128, 0, sm>>>(N, all_nodes + b, cnt);
-  }
-  float* o_nb = W.alloc<float>((size_t)total_nodes * 6);
-  int* o_nd = W.alloc<int>((size_t)total_nodes * 4);
-  int* o_refs = W.alloc<int>(n);
-  int* o_roots = W.alloc<int>(4);
-  if (!W.ok) return fail(ctx, RTB_ERR_OUT_OF_MEMORY, "BVH output");
-  k_flatten<<<blocks(total_nodes, 128), 128, 0, sm>>>(P, I, N, total_nodes, o_nb, o_nd, o_refs);
-  cudaMemcpyAsync(o_roots, h_pre.data(), roots * 4, cudaMemcpyHostToDevice, sm);
-  cudaEventRecord(ctx->ev1, sm);
-  int h_stats[4];
-  cudaMemcpyAsync(h_stats, counters + 2, sizeof(h_stats), cudaMemcpyDeviceToHost, sm);
-  e = cudaStreamSynchronize(sm);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "BVH flatten");
-  float ms = 0.0f;
-  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-  if (total_nodes != 2 * h_stats[0] - roots)
-    return fail(ctx, RTB_ERR_DEVICE_CHECK, "A binary BVH forest must contain 2 * leafCount - rootCount nodes.");
-  rtb_status s = scene_create(ctx, desc, nullptr, o_nb, o_nd, total_nodes, o_refs, n, o_roots, roots, out);
-  if (s != RTB_OK) return s;
-  if (stats) {
-    stats->node_count = total_nodes;
-    stats->root_count = roots;
-    stats->leaf_count = h_stats[0];
-    stats->max_depth = h_stats[3];
-    stats->primitive_ref_count = n;
-    stats->leaf_size = cfg->leaf_size;
-    stats->min_leaf_occupancy = h_stats[1];
-    stats->max_leaf_occupancy = h_stats[2];
-    double g = 0.0, u = 0.0, w = 0.0;
-    for (int r = 0; r < roots; ++r) {
-      u = u + h_sah[r][1];
-      w = w + h_sah[r][2];
-      g = g + h_sah[r][0];
-    }
-    stats->generalized_sah_cost = g;
-    stats->uniform_sah_cost = u;
-    stats->weighted_sah_cost = w;
-    stats->bytes = (long long)total_nodes * 24 + ((long long)total_nodes * 4 + n + roots) * 4;
-    stats->build_ms = ms;
-    stats->sequential_nodes = 0;
-  }
-  return RTB_OK;
+  return finish_build(ctx, desc, cfg, W, c, P, I, N, all_nodes, level_begin, roots, total_nodes,
+                      counters, out, stats);
 }
 
 }  // namespace rtb

@@ -96,6 +96,8 @@ SIGNATURES = {
                                    C.POINTER(C.c_void_p)]),
     "rtb_scene_build": (C.c_int, [C.c_void_p, C.POINTER(SceneDesc), C.POINTER(BuildConfig),
                                   C.POINTER(C.c_void_p), C.POINTER(BvhStats)]),
+    "rtb_scene_build_binned": (C.c_int, [C.c_void_p, C.POINTER(SceneDesc), C.POINTER(BuildConfig),
+                                         C.c_int, C.POINTER(C.c_void_p), C.POINTER(BvhStats)]),
     "rtb_scene_bvh_sizes": (C.c_int, [C.c_void_p, C.c_void_p, IP, IP, IP]),
     "rtb_scene_download_bvh": (C.c_int, [C.c_void_p, C.c_void_p, FP, IP, IP, IP]),
     "rtb_scene_destroy": (C.c_int, [C.c_void_p, C.c_void_p]),

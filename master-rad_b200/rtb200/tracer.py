@@ -139,15 +139,21 @@ class ResidentScene:
         return ResidentScene(ctx, h)
 
     @staticmethod
-    def build(ctx: Context, scene: GpuScene, config: Optional[BvhBuildConfig] = None) -> "ResidentScene":
-        """Builds the scene's BVH on the device (GpuScene.buildBvhData moved onto the GPU)."""
+    def build(ctx: Context, scene: GpuScene, config: Optional[BvhBuildConfig] = None,
+              bins: int = 0) -> "ResidentScene":
+        """Builds the scene's BVH on the device (GpuScene.buildBvhData moved onto the GPU):
+        the reference's full sweep, or with bins in 2..32 the binned object-SAH mode."""
         cfg = config if config is not None else scene.config
         d, keep = scene_desc(scene)
         bc = build_config(cfg)
         st = N.BvhStats()
         h = C.c_void_p()
-        ctx.check(ctx.lib.rtb_scene_build(ctx.handle, C.byref(d), C.byref(bc), C.byref(h),
-                                          C.byref(st)))
+        if bins:
+            ctx.check(ctx.lib.rtb_scene_build_binned(ctx.handle, C.byref(d), C.byref(bc), int(bins),
+                                                     C.byref(h), C.byref(st)))
+        else:
+            ctx.check(ctx.lib.rtb_scene_build(ctx.handle, C.byref(d), C.byref(bc), C.byref(h),
+                                              C.byref(st)))
         mean = st.primitive_ref_count / st.leaf_count if st.leaf_count else 0.0
         stats = BvhStats(st.node_count, st.root_count, st.leaf_count, st.max_depth,
                          st.primitive_ref_count, st.leaf_size, cfg.mode.name,

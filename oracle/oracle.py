@@ -35,6 +35,7 @@ def lib():
             raise FileNotFoundError(path + " (run oracle/build_oracle.py)")
         _lib = C.CDLL(path)
         _lib.orc_build_bvh.restype = C.c_int
+        _lib.orc_build_bvh_binned.restype = C.c_int
         _lib.orc_trace.restype = None
         _lib.orc_render.restype = None
         _lib.orc_cpu_render.restype = C.c_int
@@ -98,8 +99,9 @@ class Bvh:
         return topology_sha256(self.node_bounds, self.node_data, self.refs, self.roots)
 
 
-def build_bvh(scene, config=None):
-    """Builds the reference BVH for a rtb200.scene.GpuScene (or config override)."""
+def build_bvh(scene, config=None, bins=0):
+    """Builds the reference BVH for a rtb200.scene.GpuScene (or config override); with
+    bins in 2..32, the library's binned object-SAH mode instead of the full sweep."""
     cfg = config if config is not None else scene.config
     c = _Cfg(int(cfg.mode), cfg.leaf_size, cfg.traversal_weight, cfg.sphere_weight,
              cfg.box_weight, cfg.affine_sphere_weight, cfg.affine_box_weight, cfg.lam)
@@ -114,9 +116,14 @@ def build_bvh(scene, config=None):
     roots = np.zeros(4, np.int32)
     counts = np.zeros(7, np.int32)
     sah = np.zeros(3, np.float64)
-    rc = lib().orc_build_bvh(_fp(sp), ns, _fp(bx), nb, _fp(ab), nas, _fp(bb), nab, C.byref(c),
-                             _fp(nbounds), _ip(ndata), _ip(refs), _ip(roots), _ip(counts),
-                             sah.ctypes.data_as(C.POINTER(C.c_double)))
+    outs = (_fp(nbounds), _ip(ndata), _ip(refs), _ip(roots), _ip(counts),
+            sah.ctypes.data_as(C.POINTER(C.c_double)))
+    if bins:
+        rc = lib().orc_build_bvh_binned(_fp(sp), ns, _fp(bx), nb, _fp(ab), nas, _fp(bb), nab,
+                                        C.byref(c), int(bins), *outs)
+    else:
+        rc = lib().orc_build_bvh(_fp(sp), ns, _fp(bx), nb, _fp(ab), nas, _fp(bb), nab,
+                                 C.byref(c), *outs)
     if rc != 0:
         raise RuntimeError("oracle BVH build failed: %d" % rc)
     nn, nr, nref = int(counts[0]), int(counts[1]), int(counts[4])

@@ -20,6 +20,20 @@
 //   * SAH statistics        gfxlab/gpu/GpuScene.java:810-838
 // Arithmetic is IEEE double with no contraction (Java strictfp semantics); this file
 // must be compiled with -ffp-contract=off.
+//
+// orc_build_bvh_binned restates this library's binned object-SAH mode (no reference
+// counterpart; the reference builder is the full sweep above):
+//   * per axis whose centroid extent exceeds 1e-12, B bins over the node's centroid bounds,
+//     bin = min(B - 1, (int)((c - lo) * (B / extent)));
+//   * per bin, integer counts per primitive type and the float box union;
+//   * the weight of a set is ((n0 w0 + n1 w1) + n2 w2) + n3 w3 with the per-type
+//     construction weights, so sums do not depend on the order of accumulation;
+//   * plane j (1..B-1) puts bins [0, j) left; cost (A_P c_T + A_L W_L) + A_R W_R; first
+//     minimum over (axis, j); both sides non-empty;
+//   * leaf if count == 1, or count <= leafSize and !(cost < A_P W_P); a node whose
+//     centroids coincide on every axis becomes a leaf when count <= leafSize and otherwise
+//     splits at count / 2 in its current order;
+//   * children are a stable partition of the node's primitives.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -91,7 +105,18 @@ struct Config {
   int leaf_size;
   double traversal;
   double lambda;
+  int bins = 0;               // 0: full sweep; 2..32: binned mode
+  double type_weight[4] = {1.0, 1.0, 1.0, 1.0};
 };
+
+inline int type_of(int ref) { return (int)((unsigned)ref >> 30); }
+
+inline int bin_of(double c, double lo, double scale, int bins) {
+  double x = c - lo;
+  x = x * scale;
+  int b = (int)x;
+  return b < bins ? b : bins - 1;
+}
 
 struct Builder {
   std::vector<Prim>& prims;
@@ -175,7 +200,131 @@ struct Builder {
     return best;
   }
 
+  double set_weight(const long long* cnt) const {
+    double w = (double)cnt[0] * cfg.type_weight[0];
+    w = w + (double)cnt[1] * cfg.type_weight[1];
+    w = w + (double)cnt[2] * cfg.type_weight[2];
+    w = w + (double)cnt[3] * cfg.type_weight[3];
+    return w;
+  }
+
+  struct BinnedSplit {
+    bool valid = false;
+    int axis = 0, plane = 0, left_count = 0;
+    double lo = 0.0, scale = 0.0, cost = 0.0;
+  };
+
+  BinnedSplit binned_split(int start, int end, const Aabb& bounds, const Aabb& cb) {
+    const int B = cfg.bins;
+    double node_area = surface_area(bounds);
+    BinnedSplit best;
+    for (int axis = 0; axis < 3; ++axis) {
+      double ext = cb.mx[axis] - cb.mn[axis];
+      if (!(ext > 1.0e-12)) continue;
+      double scale = (double)B / ext;
+      std::vector<Aabb> box(B);
+      std::vector<long long> cnt(4 * B, 0);
+      std::vector<bool> used(B, false);
+      for (int i = start; i < end; ++i) {
+        const Prim& p = prims[i];
+        int b = bin_of(p.cen[axis], cb.mn[axis], scale, B);
+        box[b] = used[b] ? unite(box[b], p.bounds) : p.bounds;
+        used[b] = true;
+        cnt[4 * b + type_of(p.ref)]++;
+      }
+      // inclusive prefix (left) and suffix (right) over bins
+      std::vector<Aabb> lbox(B), rbox(B);
+      std::vector<long long> lc(4 * B), rc(4 * B);
+      std::vector<bool> lu(B), ru(B);
+      for (int b = 0; b < B; ++b) {
+        for (int t = 0; t < 4; ++t) lc[4 * b + t] = cnt[4 * b + t] + (b ? lc[4 * (b - 1) + t] : 0);
+        if (b && lu[b - 1]) {
+          lbox[b] = used[b] ? unite(lbox[b - 1], box[b]) : lbox[b - 1];
+          lu[b] = true;
+        } else {
+          lbox[b] = box[b];
+          lu[b] = used[b];
+        }
+      }
+      for (int b = B - 1; b >= 0; --b) {
+        for (int t = 0; t < 4; ++t)
+          rc[4 * b + t] = cnt[4 * b + t] + (b + 1 < B ? rc[4 * (b + 1) + t] : 0);
+        if (b + 1 < B && ru[b + 1]) {
+          rbox[b] = used[b] ? unite(rbox[b + 1], box[b]) : rbox[b + 1];
+          ru[b] = true;
+        } else {
+          rbox[b] = box[b];
+          ru[b] = used[b];
+        }
+      }
+      for (int j = 1; j < B; ++j) {
+        const long long* L = &lc[4 * (j - 1)];
+        const long long* R = &rc[4 * j];
+        long long nl = L[0] + L[1] + L[2] + L[3];
+        long long nr = R[0] + R[1] + R[2] + R[3];
+        if (nl == 0 || nr == 0) continue;
+        double a = node_area * cfg.traversal;
+        double bl = surface_area(lbox[j - 1]) * set_weight(L);
+        double br = surface_area(rbox[j]) * set_weight(R);
+        double cost = (a + bl) + br;
+        if (!best.valid || cost < best.cost) {
+          best.valid = true;
+          best.cost = cost;
+          best.axis = axis;
+          best.plane = j;
+          best.left_count = (int)nl;
+          best.lo = cb.mn[axis];
+          best.scale = scale;
+        }
+      }
+    }
+    return best;
+  }
+
+  int build_binned(int start, int end) {
+    Aabb bounds = prims[start].bounds;
+    Aabb cb;
+    for (int k = 0; k < 3; ++k) cb.mn[k] = cb.mx[k] = prims[start].cen[k];
+    long long cnt[4] = {0, 0, 0, 0};
+    for (int i = start; i < end; ++i) {
+      if (i > start) bounds = unite(bounds, prims[i].bounds);
+      for (int k = 0; k < 3; ++k) {
+        cb.mn[k] = std::min(cb.mn[k], prims[i].cen[k]);
+        cb.mx[k] = std::max(cb.mx[k], prims[i].cen[k]);
+      }
+      cnt[type_of(prims[i].ref)]++;
+    }
+    int count = end - start;
+    if (count == 1) return make_leaf(bounds, start, end);
+    BinnedSplit split = binned_split(start, end, bounds, cb);
+    int mid;
+    if (!split.valid) {
+      if (count <= cfg.leaf_size) return make_leaf(bounds, start, end);
+      mid = start + count / 2;
+    } else {
+      double leaf_cost = surface_area(bounds) * set_weight(cnt);
+      if (count <= cfg.leaf_size && !(split.cost < leaf_cost)) return make_leaf(bounds, start, end);
+      std::vector<Prim> left, right;
+      for (int i = start; i < end; ++i) {
+        int b = bin_of(prims[i].cen[split.axis], split.lo, split.scale, cfg.bins);
+        (b < split.plane ? left : right).push_back(prims[i]);
+      }
+      std::copy(left.begin(), left.end(), prims.begin() + start);
+      std::copy(right.begin(), right.end(), prims.begin() + start + left.size());
+      mid = start + (int)left.size();
+    }
+    int l = build_binned(start, mid);
+    int r = build_binned(mid, end);
+    Node n;
+    n.bounds = bounds;
+    n.left = l;
+    n.right = r;
+    pool.push_back(n);
+    return (int)pool.size() - 1;
+  }
+
   int build(int start, int end) {
+    if (cfg.bins > 0) return build_binned(start, end);
     Aabb bounds = prims[start].bounds;
     Aabb cb;
     for (int k = 0; k < 3; ++k) cb.mn[k] = cb.mx[k] = prims[start].cen[k];
@@ -319,15 +468,27 @@ typedef struct {
 // N = ns + nb + nas + nab.  counts: node_count, root_count, leaf_count, max_depth,
 // ref_count, min_leaf, max_leaf.  sah: generalized, uniform, weighted.
 // Returns 0 on success, negative on an unsupported configuration.
-int orc_build_bvh(const float* spheres, int ns, const float* boxes, int nb,
-                  const float* affine_sphere_bounds, int nas, const float* affine_box_bounds,
-                  int nab, const orc_build_config* cfg, float* node_bounds, int* node_data,
-                  int* refs, int* roots, int* counts, double* sah) {
+static int build_any(const float* spheres, int ns, const float* boxes, int nb,
+                     const float* affine_sphere_bounds, int nas, const float* affine_box_bounds,
+                     int nab, const orc_build_config* cfg, int bins, float* node_bounds,
+                     int* node_data, int* refs, int* roots, int* counts, double* sah) {
   if (cfg->mode < 0 || cfg->mode > 3 || cfg->leaf_size < 1) return -1;
+  if (bins != 0 && (bins < 2 || bins > 32)) return -1;
   bool weighted = cfg->mode == 1 || cfg->mode == 3;
   bool per_type = cfg->mode >= 2;
   Config c{weighted ? 1 : 0, cfg->leaf_size, cfg->traversal_weight,
            weighted ? cfg->lambda : 0.0};
+  c.bins = bins;
+  {
+    const double measured[4] = {cfg->sphere_weight, cfg->box_weight, cfg->affine_sphere_weight,
+                                cfg->affine_box_weight};
+    for (int t = 0; t < 4; ++t) {
+      if (!weighted) continue;
+      double x = measured[t] - 1.0;
+      x = c.lambda * x;
+      c.type_weight[t] = 1.0 + x;
+    }
+  }
   int total = ns + nb + nas + nab;
   std::memset(counts, 0, 7 * sizeof(int));
   sah[0] = sah[1] = sah[2] = 0.0;
@@ -414,6 +575,25 @@ int orc_build_bvh(const float* spheres, int ns, const float* boxes, int nb,
   counts[6] = max_leaf;
   if (total_summary.nodes != 2 * total_summary.leaves - (int)parts.size()) return -2;
   return 0;
+}
+
+int orc_build_bvh(const float* spheres, int ns, const float* boxes, int nb,
+                  const float* affine_sphere_bounds, int nas, const float* affine_box_bounds,
+                  int nab, const orc_build_config* cfg, float* node_bounds, int* node_data,
+                  int* refs, int* roots, int* counts, double* sah) {
+  return build_any(spheres, ns, boxes, nb, affine_sphere_bounds, nas, affine_box_bounds, nab, cfg,
+                   0, node_bounds, node_data, refs, roots, counts, sah);
+}
+
+// Binned object-SAH mode with 2..32 bins per axis (see the header of this file).
+int orc_build_bvh_binned(const float* spheres, int ns, const float* boxes, int nb,
+                         const float* affine_sphere_bounds, int nas,
+                         const float* affine_box_bounds, int nab, const orc_build_config* cfg,
+                         int bins, float* node_bounds, int* node_data, int* refs, int* roots,
+                         int* counts, double* sah) {
+  if (bins < 2 || bins > 32) return -1;
+  return build_any(spheres, ns, boxes, nb, affine_sphere_bounds, nas, affine_box_bounds, nab, cfg,
+                   bins, node_bounds, node_data, refs, roots, counts, sah);
 }
 
 }  // extern "C"
