@@ -24,7 +24,8 @@ Arms and keys of the single JSON line printed by rank 0:
   cpu_baseline  the FP64 restatement of the reference's CPU renderer on all host cores, on
             a bounded row band of the same frame (rank 0, N = 1).
   build_ms  device BVH build time of the workload's scene (tree identical to the reference
-            Java builder's).
+            Java builder's), median of 3; build.binned_ms the binned object-SAH mode (32 bins,
+            16 for the plain scene) and its SAH cost relative to the full sweep's.
 With --impl reference the line reports the reference CPU renderer (its FP64 restatement;
 the Java original cannot run here) on bounded samples of the same frame.
 With N > 1 (torchrun) every rank renders its own frames (distinct frame indices) of the same
@@ -433,6 +434,22 @@ def main():
     # ---- device build (timed by the library with CUDA events) and residency
     res = ResidentScene.build(ctx, w.scene)
     build_ms = res.stats.build_ms
+    # binned object-SAH builds of the same scene (16 bins for the plain scene, 32 otherwise):
+    # the first build warms the allocation pool; the rest are timed by the library's events
+    bins = 16 if args.workload == "plain" else 32
+    binned_ms, binned_sah = [], None
+    for i in range(4):
+        rb = ResidentScene.build(ctx, w.scene, bins=bins)
+        if i:
+            binned_ms.append(rb.stats.build_ms)
+        binned_sah = rb.stats.generalized_sah_cost
+        rb.close()
+    full_ms = []
+    for i in range(3):
+        rf = ResidentScene.build(ctx, w.scene)
+        full_ms.append(rf.stats.build_ms)
+        rf.close()
+    build_ms = statistics.median(full_ms)
     pixels = w.width * w.height
     out = torch.empty(pixels * 3, dtype=torch.float32, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -545,6 +562,11 @@ def main():
                        "l2": "flushed between frames (256 MiB write outside the events)",
                        "parallelism": "frames per rank" if world > 1 else "single GPU"},
             "build_ms": build_ms,
+            "build": {"full_sweep_ms": build_ms,
+                      "full_sweep_note": "tree identical to the reference Java builder's",
+                      "binned_ms": statistics.median(binned_ms), "bins": bins,
+                      "binned_note": "binned object SAH, identical to its CPU restatement",
+                      "binned_over_full_sah": binned_sah / res.stats.generalized_sah_cost},
             "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": pixels * 12,
                     "includes": "scene upload from pinned memory + device BVH build + render "
