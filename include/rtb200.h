@@ -243,6 +243,49 @@ RTB_API rtb_status rtb_trace_replay_static(const rtb_scene* scene, const float* 
                                            int use_bvh, int* hit_flags, float* hit_distances,
                                            int* hit_orders, int* hit_materials, float* hit_normals);
 
+/* ---- primitive-cost calibration (the counterpart of gfxlab/gpu/PrimitiveCostBenchmark.java,
+ * whose RTX 3080 results are the constants of PrimitiveCostModel.java:11-19) ----
+ * Relative cost of this library's intersection operations on the current device,
+ * normalised to the sphere test.  Operation index: 1 sphere, 2 box, 3 affine sphere,
+ * 4 affine box, 5 node AABB, 6 interior traversal (both child boxes and their order),
+ * 7 plane; 0 is the setup baseline. */
+#define RTB_CALIBRATION_MAX_PROFILES 3
+typedef struct {
+  const float* rays;     /* profiles x records x 6: origin, direction */
+  int profiles;          /* 1..3 */
+  int records;           /* a power of two */
+  const float* spheres;  /* 4 floats per record: centre, radius */
+  const float* boxes;    /* 8 floats: min (+ pad), max (+ pad) */
+  const float* affines;  /* 12 floats: inverse rows with the world centre in the 4th slot */
+  const float* planes;   /* 4 floats: unit normal, offset */
+  const float* nodes;    /* 16 floats: one child-pair node (x/y ranges of both children,
+                            z ranges, links) */
+} rtb_calibration_workload;
+
+typedef struct {
+  int blocks, threads;   /* launch shape of every timed launch (threads <= 256) */
+  int iterations;        /* per thread per observation (a multiple of sublaunches) */
+  int copies;            /* operations per iteration */
+  int sublaunches;       /* timed launches per observation, alternated with the setup */
+  int repeats, warmups;  /* paired observations per operation and profile */
+  int order_offset;      /* rotation of the operation order */
+  double max_launch_ms;  /* a longer launch aborts the calibration with RTB_ERR_LIMIT */
+} rtb_calibration_params;
+
+typedef struct {
+  int profiles;
+  double net_ns[RTB_CALIBRATION_MAX_PROFILES][8];     /* median net ns per operation */
+  double sphere_ns[RTB_CALIBRATION_MAX_PROFILES][8];  /* its paired local sphere median */
+  double ratio[RTB_CALIBRATION_MAX_PROFILES][8];      /* net / local sphere */
+  double sphere_net_ns[RTB_CALIBRATION_MAX_PROFILES];
+  double weight[8];                                   /* median ratio over the profiles */
+  long long tests_per_observation;
+} rtb_calibration_result;
+
+RTB_API rtb_status rtb_calibrate_costs(rtb_context* ctx, const rtb_calibration_workload* workload,
+                                       const rtb_calibration_params* params,
+                                       rtb_calibration_result* result);
+
 /* Host-writable abort: running persistent kernels of this context stop at their next
  * work fetch and the call returns RTB_ERR_WATCHDOG.  Cleared by the next render call. */
 RTB_API rtb_status rtb_request_abort(rtb_context* ctx);

@@ -81,6 +81,29 @@ class BatchJob(C.Structure):
                 ("rgb_device", C.c_void_p)]
 
 
+CALIBRATION_MAX_PROFILES = 3  # RTB_CALIBRATION_MAX_PROFILES
+
+
+class CalibrationWorkload(C.Structure):
+    _fields_ = [("rays", FP), ("profiles", C.c_int), ("records", C.c_int), ("spheres", FP),
+                ("boxes", FP), ("affines", FP), ("planes", FP), ("nodes", FP)]
+
+
+class CalibrationParams(C.Structure):
+    _fields_ = [("blocks", C.c_int), ("threads", C.c_int), ("iterations", C.c_int),
+                ("copies", C.c_int), ("sublaunches", C.c_int), ("repeats", C.c_int),
+                ("warmups", C.c_int), ("order_offset", C.c_int), ("max_launch_ms", C.c_double)]
+
+
+class CalibrationResult(C.Structure):
+    _fields_ = [("profiles", C.c_int),
+                ("net_ns", (C.c_double * 8) * CALIBRATION_MAX_PROFILES),
+                ("sphere_ns", (C.c_double * 8) * CALIBRATION_MAX_PROFILES),
+                ("ratio", (C.c_double * 8) * CALIBRATION_MAX_PROFILES),
+                ("sphere_net_ns", C.c_double * CALIBRATION_MAX_PROFILES),
+                ("weight", C.c_double * 8), ("tests_per_observation", C.c_longlong)]
+
+
 class BatchTuning(C.Structure):
     _fields_ = [("threads_per_block", C.c_int), ("job_order", C.c_int)]
 
@@ -109,6 +132,9 @@ SIGNATURES = {
                                     C.POINTER(RenderParams), C.c_void_p, C.c_void_p]),
     "rtb_last_frame_stats": (C.c_int, [C.c_void_p, C.POINTER(FrameStats)]),
     "rtb_request_abort": (C.c_int, [C.c_void_p]),
+    "rtb_calibrate_costs": (C.c_int, [C.c_void_p, C.POINTER(CalibrationWorkload),
+                                      C.POINTER(CalibrationParams),
+                                      C.POINTER(CalibrationResult)]),
     "rtb_trace_replay_static": (C.c_int, [C.c_void_p, FP, C.c_int, C.c_int, IP, FP, IP, IP, FP]),
     "rtb_batch_create": (C.c_int, [C.c_void_p, C.POINTER(BatchJob), C.c_int, C.POINTER(BatchTuning),
                                    C.POINTER(C.c_void_p)]),
