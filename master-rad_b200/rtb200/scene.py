@@ -48,6 +48,22 @@ class PrimitiveCostModel:
     INTERIOR_TRAVERSAL = 1.275576713
 
 
+def traversal_work(aabb_tests, sphere_tests, box_tests, plane_tests, affine_sphere_tests,
+                   affine_box_tests, model=PrimitiveCostModel) -> float:
+    """TraversalWorkMetric.cost (TraversalWorkMetric.java:14-38): one cost term per
+    measured AABB test and per primitive test, weighted by the cost model (any object with
+    the PrimitiveCostModel attributes); shading, memory and divergence are left out."""
+    return (model.NODE_AABB * aabb_tests + model.SPHERE * sphere_tests + model.BOX * box_tests
+            + model.PLANE * plane_tests + model.AFFINE_SPHERE * affine_sphere_tests
+            + model.AFFINE_BOX * affine_box_tests)
+
+
+def frame_traversal_work(stats, model=PrimitiveCostModel) -> float:
+    """traversal_work of a FrameStats (TraversalWorkMetric.cost(FrameStats))."""
+    return traversal_work(stats.aabb_tests, stats.sphere_tests, stats.box_tests, stats.plane_tests,
+                          stats.affine_sphere_tests, stats.affine_box_tests, model)
+
+
 class BvhBuildMode(enum.IntEnum):
     """BvhBuildMode.java:4-44 (ordinals are part of the C ABI)."""
     UNIFORM_SAH = 0

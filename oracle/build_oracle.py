@@ -69,7 +69,7 @@ def build_reference(force=False):
         extract_reference_kernel(src)
     outs = {}
     for name, flags in (("fmad", ["-fmad=true"]), ("nofmad", ["-fmad=false"]),
-                        ("metrics", ["-fmad=true", "-DGFXLAB_RENDER_METRICS=1"])):
+                        ("metrics", ["-fmad=false", "-DGFXLAB_RENDER_METRICS=1"])):
         out = os.path.join(ref_dir, "libref_%s.so" % name)
         if force or _stale(out, [src, harness]):
             _run([NVCC] + ARCH + ["-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",

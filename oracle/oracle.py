@@ -236,6 +236,22 @@ def ref_render(workload, bvh=None, use_bvh=True, warmup=0, frames=1, variant="fm
     return out.reshape(-1, 3), ms.value
 
 
+def ref_render_stats(workload, bvh=None, use_bvh=True):
+    """One frame of the reference's renderKernel from its metrics build (no contraction,
+    GFXLAB_RENDER_METRICS): (image (H*W,3), the 14 frame counters of K:30-43)."""
+    w = workload
+    sa = _SceneArgs(w.scene, bvh, use_bvh)
+    out = np.zeros(3 * w.width * w.height, np.float32)
+    stats = np.zeros(14, np.uint64)
+    rc = ref_lib("metrics").ref_render_stats(
+        *sa.args(), _fp(_f32(w.camera.packed())), _fp(_f32(w.scene.background)),
+        _ip(_render_params(w)), C.c_ulonglong(w.frame_seed), _fp(out),
+        stats.ctypes.data_as(C.POINTER(C.c_ulonglong)))
+    if rc != 0:
+        raise RuntimeError("reference metrics render failed: %d" % rc)
+    return out.reshape(-1, 3), stats
+
+
 def cpu_render(workload, frames=None, rows=None, threads=0, seed=0x68EFD508E309A865):
     """FP64 restatement of the reference CPU renderer; returns (H_rows*W, 3) doubles."""
     w = workload

@@ -143,11 +143,11 @@ int ref_trace(const float* const* arrays, const int* counts, const int* bvh_ints
 // timed frames (ms, summed) in *kernel_ms and the last frame's image in rgb (3 floats
 // per pixel, may be null).  camera: pos, forward, right, up; params: width, height,
 // spp, max_depth, frame_index.
-int ref_render(const float* const* arrays, const int* counts, const int* bvh_ints,
-               const float* node_bounds, const int* node_data, const int* refs, const int* roots,
-               const float* camera, const float* background, const int* params,
-               unsigned long long frame_seed, int warmup, int frames, float* rgb,
-               double* kernel_ms) {
+static int render_frames(const float* const* arrays, const int* counts, const int* bvh_ints,
+                         const float* node_bounds, const int* node_data, const int* refs,
+                         const int* roots, const float* camera, const float* background,
+                         const int* params, unsigned long long frame_seed, int warmup, int frames,
+                         float* rgb, double* kernel_ms, unsigned long long* stats) {
   DevScene s;
   int rc = make_scene(&s, arrays, counts, bvh_ints, node_bounds, node_data, refs, roots);
   int width = params[0], height = params[1], spp = params[2], max_depth = params[3];
@@ -156,6 +156,7 @@ int ref_render(const float* const* arrays, const int* counts, const int* bvh_int
   unsigned long long* d_stats = nullptr;
   if (!rc && cudaMalloc(&d_out, (size_t)width * height * 12) != cudaSuccess) rc = -1;
   if (!rc && cudaMalloc(&d_stats, 14 * 8) != cudaSuccess) rc = -1;
+  if (!rc) cudaMemset(d_stats, 0, 14 * 8);
   int tw, th, cols, rows;
   tile_layout(width, height, 262144, &tw, &th, &cols, &rows);
   cudaEvent_t e0, e1;
@@ -178,7 +179,7 @@ int ref_render(const float* const* arrays, const int* counts, const int* bvh_int
             s.aspheres, s.counts[3], s.aboxes, s.counts[4], s.node_bounds, s.node_count,
             s.node_data, s.refs, s.ref_count, s.roots, s.root_count, s.use_bvh, s.materials,
             s.counts[5], background[0], background[1], background[2], max_depth, frame_index,
-            frame_seed, so, spp, d_stats, 0);
+            frame_seed, so, spp, d_stats, stats ? 1 : 0);
       }
     }
     if (cudaGetLastError() != cudaSuccess) rc = -2;
@@ -192,6 +193,7 @@ int ref_render(const float* const* arrays, const int* counts, const int* bvh_int
   }
   if (!rc && cudaDeviceSynchronize() != cudaSuccess) rc = -3;
   if (!rc && rgb) cudaMemcpy(rgb, d_out, (size_t)width * height * 12, cudaMemcpyDeviceToHost);
+  if (!rc && stats) cudaMemcpy(stats, d_stats, 14 * 8, cudaMemcpyDeviceToHost);
   if (kernel_ms) *kernel_ms = total;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -199,6 +201,26 @@ int ref_render(const float* const* arrays, const int* counts, const int* bvh_int
   cudaFree(d_stats);
   free_scene(&s);
   return rc;
+}
+
+int ref_render(const float* const* arrays, const int* counts, const int* bvh_ints,
+               const float* node_bounds, const int* node_data, const int* refs, const int* roots,
+               const float* camera, const float* background, const int* params,
+               unsigned long long frame_seed, int warmup, int frames, float* rgb,
+               double* kernel_ms) {
+  return render_frames(arrays, counts, bvh_ints, node_bounds, node_data, refs, roots, camera,
+                       background, params, frame_seed, warmup, frames, rgb, kernel_ms, nullptr);
+}
+
+// One frame with the kernel's metrics enabled (a build with GFXLAB_RENDER_METRICS): the 14
+// frame counters (K:30-43) summed over the frame's launches.
+int ref_render_stats(const float* const* arrays, const int* counts, const int* bvh_ints,
+                     const float* node_bounds, const int* node_data, const int* refs,
+                     const int* roots, const float* camera, const float* background,
+                     const int* params, unsigned long long frame_seed, float* rgb,
+                     unsigned long long* stats) {
+  return render_frames(arrays, counts, bvh_ints, node_bounds, node_data, refs, roots, camera,
+                       background, params, frame_seed, 0, 1, rgb, nullptr, stats);
 }
 
 }  // extern "C"

@@ -1,0 +1,83 @@
+"""Counter parity with the reference kernel's metrics build (GFXLAB_RENDER_METRICS, the 14
+frame counters of GpuKernelSources.java:30-43, built here without contraction like this
+library) and the traversal work metric (TraversalWorkMetric.java:14-38).
+
+Where the work does not depend on the tree walk the counts are equal: rays / path segments,
+plane tests and, in linear mode, every per-type primitive test.  In BVH mode this library
+walks its own 64-byte child-pair nodes (child boxes tested at the parent, leaves folded into
+it): its node visits are the reference's plus one per ray (the synthetic top node over the
+roots), and it tests a far leaf child even when the near leaf's hit already excludes it
+(about 5 % more primitive tests on the heterogeneous scene; skipping them measured slower,
+the check costs more inside the divergent leaf loop than the tests it saves)."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from rtb200 import synth
+from rtb200.scene import PrimitiveCostModel, frame_traversal_work, traversal_work
+from rtb200.tracer import GpuRayTracer
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ["rays", "aabb", "prim", "sphere", "box", "plane", "asphere", "abox", "overflow",
+         "max_stack", "internal", "leaf", "homogeneous", "mixed"]
+
+
+def _small(w, size=96, spp=2):
+    return dataclasses.replace(w, width=size, height=size, spp=spp)
+
+
+def _ours(w, use_bvh):
+    with GpuRayTracer(w.width, w.height, w.spp, bvh_traversal=use_bvh, collect_metrics=True) as tr:
+        img = tr.render_sample(None, w.scene, w.camera, w.max_depth, w.frame_index, w.frame_seed)
+        st = tr.last_frame_stats()
+    c = np.array([st.rays, st.aabb_tests, st.primitive_tests, st.sphere_tests, st.box_tests,
+                  st.plane_tests, st.affine_sphere_tests, st.affine_box_tests, st.stack_overflows,
+                  st.max_stack_size, st.internal_node_visits, st.leaf_node_visits,
+                  st.homogeneous_leaf_node_visits, st.mixed_leaf_node_visits], np.int64)
+    return np.asarray(img).reshape(-1, 3), c, st
+
+
+@pytest.mark.parametrize("name", ["plain", "hetero"])
+def test_linear_mode_counters_equal_the_reference(name):
+    w = _small(synth.plain_workload() if name == "plain" else synth.hetero_workload(), 48, 1)
+    img, ours, _ = _ours(w, use_bvh=False)
+    ref_img, ref = oracle.ref_render_stats(w, use_bvh=False)
+    np.testing.assert_array_equal(img.view(np.int32), ref_img.view(np.int32))
+    for k in ("rays", "prim", "sphere", "box", "plane", "asphere", "abox"):
+        i = NAMES.index(k)
+        assert ours[i] == int(ref[i]), (k, ours[i], int(ref[i]))
+
+
+@pytest.mark.parametrize("name", ["plain", "hetero"])
+def test_bvh_mode_counters_and_traversal_work(name):
+    w = _small(synth.plain_workload() if name == "plain" else synth.hetero_workload())
+    bvh = oracle.build_bvh(w.scene)
+    img, ours, st = _ours(w, use_bvh=True)
+    ref_img, ref = oracle.ref_render_stats(w, bvh=bvh, use_bvh=True)
+    np.testing.assert_array_equal(img.view(np.int32), ref_img.view(np.int32))
+    ref = ref.astype(np.int64)
+    # the same paths: the same segments and plane tests
+    for k in ("rays", "plane"):
+        i = NAMES.index(k)
+        assert ours[i] == ref[i], (k, ours[i], ref[i])
+    assert ours[NAMES.index("overflow")] == 0 and ref[NAMES.index("overflow")] == 0
+    # node visits: the reference's, plus the synthetic top node once per ray (one root)
+    i, r = NAMES.index("internal"), NAMES.index("rays")
+    assert abs(int(ours[i]) - int(ref[i]) - int(ours[r])) <= 0.001 * ref[i], (ours[i], ref[i], ours[r])
+    # bounded-primitive tests: the same leaves reached, within the same order of magnitude
+    p = NAMES.index("prim")
+    ours_bvh = ours[p] - ours[NAMES.index("plane")]
+    ref_bvh = ref[p] - ref[NAMES.index("plane")]
+    assert ref_bvh <= ours_bvh <= 1.1 * ref_bvh, (ours_bvh, ref_bvh)
+    work = frame_traversal_work(st)
+    ref_work = traversal_work(*[ref[NAMES.index(k)] for k in
+                                ("aabb", "sphere", "box", "plane", "asphere", "abox")],
+                              model=PrimitiveCostModel)
+    assert work > 0 and ref_work > 0
+    print("\n%s counters (ours / reference):" % name)
+    for k, a, b in zip(NAMES, ours, ref):
+        print("  %-12s %12d %12d" % (k, a, b))
+    print("  traversal work %.4g / %.4g" % (work, ref_work))
