@@ -335,6 +335,7 @@ class GpuScene:
         self._mat_rows: list = []
         self._mat_index: dict = {}
         self._chunks = {k: [] for k in ("sphere", "box", "plane", "asphere", "abox")}
+        self._plane_grids = {}
         self._cache: dict = {}
         self.revision = 0
 
@@ -426,6 +427,44 @@ class GpuScene:
 
     def add_plane(self, point, normal, material: MaterialData) -> "GpuScene":
         return self.add_planes([point], [normal], [self.register_material(material)])
+
+    def add_grid_plane(self, point, normal, e, f, cell_size, line_width, surface: MaterialData,
+                       cell: MaterialData, line: MaterialData) -> "GpuScene":
+        """A plane carrying the kernel's grid material (GridData K:128-134, loadPlane
+        K:233-249, choosePlaneMaterialIndex K:251-269): a hit point's coordinates (u, v) in
+        the in-plane basis (e, f), measured from ``point``, select ``line`` within
+        line_width of a cell edge (cells of cell_size) and ``cell`` elsewhere.  GpuScene
+        itself writes no grid (GpuScene.java:548-569); the record layout is the kernel's."""
+        index = self.plane_count
+        self.add_plane(point, normal, surface)
+        e = np.asarray(e, np.float64)
+        f = np.asarray(f, np.float64)
+        ee, ff, ef = float(e @ e), float(f @ f), float(e @ f)
+        sin_sq = 1.0 - ef * ef / (ee * ff)
+        if not (ee > 0.0 and ff > 0.0 and sin_sq > 0.0):
+            raise ValueError("Grid basis vectors must be non-zero and not parallel.")
+        cs = np.asarray(cell_size, np.float64).reshape(2)
+        lw = np.asarray(line_width, np.float64).reshape(2)
+        if not (np.all(cs > 0.0) and np.all(lw >= 0.0)):
+            raise ValueError("Grid cell sizes must be positive and line widths non-negative.")
+        rec = np.zeros(FLOATS_PER_PLANE - 4, np.float64)  # slots 4..25
+        rec[0:3] = point
+        rec[3:6] = e
+        rec[6:9] = f
+        rec[9], rec[10] = ee, ff
+        # (u, v) solve rel = u e + v f: b_e = rel.e / |e|^2 = u + v ef/|e|^2 and
+        # b_f = u ef/|f|^2 + v, so the kernel's e_f is ef/|f|^2 and f_e is ef/|e|^2
+        rec[11], rec[12] = ef / ff, ef / ee
+        rec[13] = sin_sq
+        rec[14] = 1.0
+        rec[15:17] = cs
+        rec[17:19] = lw
+        rec[20] = self.register_material(cell)
+        rec[21] = self.register_material(line)
+        _require_finite_f32(rec.reshape(1, -1), "Grid plane record")
+        self._plane_grids[index] = rec
+        self._invalidate()
+        return self
 
     def _add_affine(self, kind, inverse, centre, bmin, bmax, material_ids, label):
         inv = np.asarray(inverse, dtype=np.float64).reshape(-1, 3, 3)
@@ -550,6 +589,10 @@ class GpuScene:
                 out[:, 18 + 5] = self._cat("plane", 2)
                 out[:, 18 + 6] = -1.0
                 out[:, 18 + 7] = -1.0
+                for i, rec in self._plane_grids.items():
+                    surface = out[i, 18 + 5]
+                    out[i, 4:] = rec
+                    out[i, 18 + 5] = surface
             self._cache["plane"] = out.reshape(-1)
         return self._cache["plane"]
 
