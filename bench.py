@@ -160,13 +160,19 @@ def algorithmic_bytes(counters, hits):
 
 
 def cpu_baseline(w, rows, threads=0):
+    """The FP64 CPU renderer on the centre `rows` rows of the frame: (Msamples/s, seconds,
+    samples, the rows' mean radiance (rows*width, 3), first row)."""
     from oracle import oracle
     r0 = w.height // 2 - rows // 2
     t0 = time.perf_counter()
-    oracle.cpu_render(w, frames=w.spp, rows=(r0, r0 + rows), threads=threads)
+    img = oracle.cpu_render(w, frames=w.spp, rows=(r0, r0 + rows), threads=threads)
     dt = time.perf_counter() - t0
     samples = rows * w.width * w.spp
-    return samples / dt / 1e6, dt, samples
+    return samples / dt / 1e6, dt, samples, img, r0
+
+
+def band_rmse(a, b):
+    return float(np.sqrt(np.mean((np.asarray(a, np.float64) - np.asarray(b, np.float64)) ** 2)))
 
 
 # Ranks render disjoint frame ranges of the same workload: rank r's frames start at
@@ -215,7 +221,7 @@ def run_reference(args):
         cpu_baseline(w, rows, threads)
     vals, times = [], []
     for _ in range(args.steps):
-        v, dt, samples = cpu_baseline(w, rows, threads)
+        v, dt, samples, _, _ = cpu_baseline(w, rows, threads)
         vals.append(v)
         times.append(dt)
     value = sum(rows * w.width * w.spp for _ in times) / sum(times) / 1e6
@@ -501,6 +507,7 @@ def main():
     if world > 1:
         dist.barrier()
     clock_info = clocks.stop()
+    last_frame = out.cpu().numpy().reshape(-1, 3)  # an independent frame, for the noise floor
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = float(sum(step_ms))
     total_ms = max_over_ranks(total_ms)
@@ -545,11 +552,22 @@ def main():
         if world == 1 and not args.no_cpu_baseline:
             rows = 80 if args.workload == "hetero" else 16
             rows = min(rows, w.height)
-            v, dt, samples = cpu_baseline(w, rows)
+            v, dt, samples, cpu_img, r0 = cpu_baseline(w, rows)
             cpu = {"value": v, "unit": "Msamples/s", "cores": os.cpu_count(), "kind": "port",
                    "sample": "%d centre rows x %d px x %d spp of the same frame (%d samples, "
                              "%.1f s), FP64 restatement of the reference CPU renderer"
                              % (rows, w.width, w.spp, samples, dt)}
+            # RMSE of the GPU frame against the FP64 CPU render on the same rows, beside the
+            # RMSE between two GPU frames (the Monte Carlo noise floor at this spp)
+            band = slice(r0 * w.width, (r0 + rows) * w.width)
+            gpu_a = host_img.reshape(-1, 3)[band]
+            gpu_b = last_frame[band]
+            rm = band_rmse(gpu_a, cpu_img)
+            floor = band_rmse(gpu_a, gpu_b)
+            cpu["rmse_vs_gpu"] = {"rmse": rm, "gpu_noise_floor_rmse": floor,
+                                  "ratio": rm / floor if floor > 0 else None,
+                                  "mean_radiance_gpu": float(np.mean(gpu_a)),
+                                  "mean_radiance_cpu": float(np.mean(cpu_img))}
         line = {
             "metric": "Msamples/s", "value": value, "unit": "Msamples/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,

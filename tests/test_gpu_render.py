@@ -107,3 +107,24 @@ def test_metrics_counters():
     assert st.leaf_node_visits == st.homogeneous_leaf_node_visits + st.mixed_leaf_node_visits
     assert st.plane_tests == 6 * st.rays
     assert st.aabb_tests == 2 * st.internal_node_visits
+
+
+@pytest.mark.parametrize("name", ["plain", "hetero"])
+def test_rmse_vs_fp64_cpu_renderer(name):
+    """The GPU image against the FP64 restatement of the reference's CPU renderer (its own
+    sampler and jitter, so the agreement is statistical): the RMSE between them stays at the
+    Monte Carlo noise floor, measured as the RMSE between two GPU frames, and the mean
+    radiance agrees."""
+    import dataclasses
+    base = synth.plain_workload() if name == "plain" else synth.hetero_workload()
+    w = dataclasses.replace(base, width=64, height=48, spp=64,
+                            camera=synth.camera_looking_z(base.camera.position, 64 / 48))
+    a, _ = _render(w, None)
+    b, _ = _render(dataclasses.replace(w, frame_index=w.frame_index + 1), None)
+    cpu = oracle.cpu_render(w)
+    rmse = float(np.sqrt(np.mean((a.astype(np.float64) - cpu) ** 2)))
+    floor = float(np.sqrt(np.mean((a.astype(np.float64) - b) ** 2)))
+    print("\n%s: rmse vs FP64 CPU %.4g, GPU noise floor %.4g, ratio %.3f, means %.4g / %.4g"
+          % (name, rmse, floor, rmse / floor, a.mean(), cpu.mean()))
+    assert rmse < 1.3 * floor
+    assert abs(a.mean() - cpu.mean()) < 0.05 * cpu.mean()
