@@ -74,8 +74,8 @@ typedef struct {
 } rtb_bvh_desc;
 
 /* BvhBuildConfig (gfxlab/gpu/BvhBuildConfig.java:6-15); mode is a BvhBuildMode ordinal
- * (0 UNIFORM_SAH, 1 WEIGHTED_SAH, 2 PER_TYPE_SAH, 3 PER_TYPE_WEIGHTED_SAH; the SBVH and
- * rotation modes return RTB_ERR_UNSUPPORTED). */
+ * (0 UNIFORM_SAH, 1 WEIGHTED_SAH, 2 PER_TYPE_SAH, 3 PER_TYPE_WEIGHTED_SAH, 6 SAH_ROTATIONS,
+ * 7 WEIGHTED_SAH_ROTATIONS; the SBVH modes 4 and 5 return RTB_ERR_UNSUPPORTED). */
 typedef struct {
   int mode;
   int leaf_size;
@@ -83,6 +83,18 @@ typedef struct {
   double sphere_weight, box_weight, affine_sphere_weight, affine_box_weight;
   double lambda;
 } rtb_build_config;
+
+/* BvhBuildOptions (gfxlab/gpu/BvhBuildOptions.java:4-33); defaults 128, 2.0, 8, 16, 1e-5, 4.
+ * The device builders read rotation_passes (rotation modes); the spatial-split fields
+ * belong to the SBVH modes. */
+typedef struct {
+  int spatial_bins;
+  double max_reference_multiplier;
+  int max_splits_per_primitive;
+  int min_spatial_references;
+  double spatial_overlap_threshold;
+  int rotation_passes;
+} rtb_build_options;
 
 /* GpuScene.BvhStats (GpuScene.java:113-133) plus the device build time. */
 typedef struct {
@@ -92,6 +104,7 @@ typedef struct {
   long long bytes;
   double build_ms;          /* CUDA-event time of the device build */
   int sequential_nodes;     /* nodes whose split needed the exact sequential weight order */
+  int rotation_count;       /* BvhStats.rotationCount of the rotation modes */
 } rtb_bvh_stats;
 
 /* GpuCamera (gfxlab/gpu/GpuCamera.java): direction = forward + right u + up v. */
@@ -140,6 +153,12 @@ RTB_API rtb_status rtb_scene_upload(rtb_context* ctx, const rtb_scene_desc* desc
                             rtb_scene** out);
 RTB_API rtb_status rtb_scene_build(rtb_context* ctx, const rtb_scene_desc* desc,
                            const rtb_build_config* config, rtb_scene** out, rtb_bvh_stats* stats);
+/* rtb_scene_build with explicit BvhBuildOptions (GpuSceneBuilder.from(scene, config,
+ * options), GpuSceneBuilder.java:19-35); options NULL means the defaults. */
+RTB_API rtb_status rtb_scene_build_with_options(rtb_context* ctx, const rtb_scene_desc* desc,
+                                        const rtb_build_config* config,
+                                        const rtb_build_options* options, rtb_scene** out,
+                                        rtb_bvh_stats* stats);
 /* Binned object SAH on the device: 2..32 centroid bins per axis, the configuration's
  * per-type weights, counts accumulated by warp-aggregated atomics, FP64 split selection
  * from integer bin counts.  No counterpart in the reference (its builder is the full sweep

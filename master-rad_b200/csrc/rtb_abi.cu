@@ -192,6 +192,20 @@ rtb_status rtb_scene_build(rtb_context* ctx, const rtb_scene_desc* desc, const r
   return s;
 }
 
+rtb_status rtb_scene_build_with_options(rtb_context* ctx, const rtb_scene_desc* desc,
+                                        const rtb_build_config* config,
+                                        const rtb_build_options* options, rtb_scene** out,
+                                        rtb_bvh_stats* stats) {
+  if (!ctx) return RTB_ERR_INVALID_ARGUMENT;
+  Guard g(ctx);
+  auto t0 = Clock::now();
+  ctx_acquire(ctx, ctx->stream);
+  rtb_status s = build_bvh_options(ctx, desc, config, options, out, stats);
+  ctx_release(ctx, ctx->stream);
+  if (s == RTB_OK) ctx->last.upload_ns = ns_since(t0);
+  return s;
+}
+
 rtb_status rtb_scene_build_binned(rtb_context* ctx, const rtb_scene_desc* desc,
                                   const rtb_build_config* config, int bins, rtb_scene** out,
                                   rtb_bvh_stats* stats) {

@@ -236,15 +236,168 @@ __global__ void k_sides(IdxSet I, const Nodes N, const int* key, const int* leve
 
 
 
+// ---- BvhRotator (GpuScene.java:968-1057) on the device
+//
+// A pass visits the tree bottom-up; at each interior node it compares the current node
+// with the four rotations that swap a grandchild with the uncle, by areaCost (surface area
+// times c_T per interior node plus surface area times the leaf's sequential weight sum per
+// leaf), and keeps the first one cheaper by more than 1e-12.  The decision at a node only
+// reads its own subtree, which the deeper levels have already settled, so each level runs
+// in parallel.  The reference recomputes areaCost recursively for every candidate; here each
+// node keeps its settled subtree's cost, and a candidate's cost adds the same terms in the
+// same order ((A_node c_T + cost(left)) + cost(right)), so every comparison is the
+// reference's to the bit.  A rotation reuses the child slot it restructures.
+
+// Breadth-first levels of the current tree: children of the frontier.
+__global__ void k_next_level(const Nodes N, const int* frontier, int k, int* next, int* next_count) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= k) return;
+  int node = frontier[g];
+  if (N.leaf[node]) return;
+  int q = atomicAdd(next_count, 2);
+  next[q] = N.left[node];
+  next[q + 1] = N.right[node];
+}
+
+__global__ void k_leaf_area_cost(const Prims P, IdxSet I, const Nodes N, const int* nodes, int k,
+                                 double* rcost) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= k) return;
+  int node = nodes[g];
+  if (!N.leaf[node]) return;
+  double w = 0.0;
+  for (int j = N.start[node]; j < N.end[node]; ++j) w = w + P.w[current_prim(I.a, N.order_axis[node], j)];
+  rcost[node] = surface_area(N.bounds[node]) * w;
+}
+
+__device__ __forceinline__ Box box_union(const Box& a, const Box& b) { return BoxUnion()(a, b); }
+
+__global__ void k_rotate_level(Nodes N, const int* nodes, int k, double traversal, double* rcost,
+                               int* rotations) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= k) return;
+  int n = nodes[g];
+  if (N.leaf[n]) return;
+  const double eps = 1.0e-12;
+  int L = N.left[n], R = N.right[n];
+  double top = surface_area(N.bounds[n]) * traversal;
+  double x = top + rcost[L];
+  double best = x + rcost[R];
+  int choice = 0;
+  double inner_best = 0.0;
+  if (!N.leaf[L]) {
+    int a = N.left[L], b = N.right[L], c = R;
+    // join(a, join(b, c))
+    double in1 = surface_area(box_union(N.bounds[b], N.bounds[c])) * traversal;
+    in1 = in1 + rcost[b];
+    in1 = in1 + rcost[c];
+    double c1 = top + rcost[a];
+    c1 = c1 + in1;
+    if (c1 < best - eps) {
+      best = c1;
+      choice = 1;
+      inner_best = in1;
+    }
+    // join(b, join(a, c))
+    double in2 = surface_area(box_union(N.bounds[a], N.bounds[c])) * traversal;
+    in2 = in2 + rcost[a];
+    in2 = in2 + rcost[c];
+    double c2 = top + rcost[b];
+    c2 = c2 + in2;
+    if (c2 < best - eps) {
+      best = c2;
+      choice = 2;
+      inner_best = in2;
+    }
+  }
+  if (!N.leaf[R]) {
+    int a = L, b = N.left[R], c = N.right[R];
+    // join(join(a, c), b)
+    double in3 = surface_area(box_union(N.bounds[a], N.bounds[c])) * traversal;
+    in3 = in3 + rcost[a];
+    in3 = in3 + rcost[c];
+    double c3 = top + in3;
+    c3 = c3 + rcost[b];
+    if (c3 < best - eps) {
+      best = c3;
+      choice = 3;
+      inner_best = in3;
+    }
+    // join(join(a, b), c)
+    double in4 = surface_area(box_union(N.bounds[a], N.bounds[b])) * traversal;
+    in4 = in4 + rcost[a];
+    in4 = in4 + rcost[b];
+    double c4 = top + in4;
+    c4 = c4 + rcost[c];
+    if (c4 < best - eps) {
+      best = c4;
+      choice = 4;
+      inner_best = in4;
+    }
+  }
+  if (choice == 1 || choice == 2) {
+    int a = N.left[L], b = N.right[L], c = R;
+    int outer = choice == 1 ? a : b, p = choice == 1 ? b : a;
+    N.left[n] = outer;
+    N.right[n] = L;
+    N.left[L] = p;
+    N.right[L] = c;
+    N.bounds[L] = box_union(N.bounds[p], N.bounds[c]);
+    rcost[L] = inner_best;
+  } else if (choice == 3 || choice == 4) {
+    int a = L, b = N.left[R], c = N.right[R];
+    int q = choice == 3 ? c : b, outer = choice == 3 ? b : c;
+    N.left[n] = R;
+    N.right[n] = outer;
+    N.left[R] = a;
+    N.right[R] = q;
+    N.bounds[R] = box_union(N.bounds[a], N.bounds[q]);
+    rcost[R] = inner_best;
+  }
+  rcost[n] = best;
+  if (choice) atomicAdd(rotations, 1);
+}
+
+// Breadth-first levels of the tree under `roots`: nodes level by level in `all_nodes`,
+// level starts in level_begin.  Returns false on a CUDA error.
+bool tree_levels(const Nodes& N, int roots, int* all_nodes, int* counter, std::vector<int>& level_begin,
+                 cudaStream_t sm) {
+  std::vector<int> h(roots);
+  for (int r = 0; r < roots; ++r) h[r] = r;
+  cudaMemcpyAsync(all_nodes, h.data(), roots * 4, cudaMemcpyHostToDevice, sm);
+  level_begin.assign(1, 0);
+  int begin = 0, k = roots;
+  while (k > 0) {
+    level_begin.push_back(begin + k);
+    cudaMemsetAsync(counter, 0, 4, sm);
+    k_next_level<<<blocks(k), 256, 0, sm>>>(N, all_nodes + begin, k, all_nodes + begin + k, counter);
+    int next = 0;
+    cudaMemcpyAsync(&next, counter, 4, cudaMemcpyDeviceToHost, sm);
+    if (cudaStreamSynchronize(sm) != cudaSuccess) return false;
+    begin += k;
+    k = next;
+  }
+  return true;
+}
+
 }  // namespace
 
 rtb_status build_bvh(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_build_config* cfg,
                      rtb_scene** out, rtb_bvh_stats* stats) {
+  return build_bvh_options(ctx, desc, cfg, nullptr, out, stats);
+}
+
+rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_build_config* cfg,
+                             const rtb_build_options* options, rtb_scene** out, rtb_bvh_stats* stats) {
   if (!out) return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "null argument");
   BuildCfg c;
   bool per_type = false;
-  rtb_status st = build_setup(ctx, desc, cfg, c, per_type);
+  rtb_status st = build_setup(ctx, desc, cfg, c, per_type, true);
   if (st != RTB_OK) return st;
+  int rotation_passes = options ? options->rotation_passes : 4;  // BvhBuildOptions.defaults
+  bool rotate = cfg->mode == 6 || cfg->mode == 7;
+  if (rotate && rotation_passes < 1)
+    return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "rotationPasses must be positive.");
   if (stats) *stats = rtb_bvh_stats{};
   if (c.total == 0) {
     rtb_status s = scene_create(ctx, desc, nullptr, nullptr, nullptr, 0, nullptr, 0, nullptr, 0, out);
@@ -386,8 +539,43 @@ rtb_status build_bvh(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_bui
     k = next;
     level++;
   }
-  return finish_build(ctx, desc, cfg, W, c, P, I, N, all_nodes, level_begin, roots, total_nodes,
-                      counters, out, stats);
+  int rotation_count = 0;
+  if (rotate) {
+    double* rcost = W.alloc<double>(cap);
+    int* rot = W.alloc<int>(2);
+    if (!W.ok) return fail(ctx, RTB_ERR_OUT_OF_MEMORY, "BVH rotation workspace");
+    bool leaves_done = false;
+    for (int pass = 0; pass < rotation_passes; ++pass) {
+      if (!tree_levels(N, roots, all_nodes, rot + 1, level_begin, sm))
+        return cuda_fail(ctx, cudaGetLastError(), "BVH levels");
+      int levels = (int)level_begin.size() - 1;
+      if (!leaves_done) {
+        k_leaf_area_cost<<<blocks(total_nodes), 256, 0, sm>>>(P, I, N, all_nodes, total_nodes, rcost);
+        leaves_done = true;
+      }
+      cudaMemsetAsync(rot, 0, 4, sm);
+      for (int L = levels - 1; L >= 0; --L) {
+        int b = level_begin[L], cnt = level_begin[L + 1] - b;
+        k_rotate_level<<<blocks(cnt), 256, 0, sm>>>(N, all_nodes + b, cnt, c.traversal, rcost, rot);
+      }
+      int h_rot = 0;
+      cudaMemcpyAsync(&h_rot, rot, 4, cudaMemcpyDeviceToHost, sm);
+      cudaError_t e = cudaStreamSynchronize(sm);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "BVH rotation pass");
+      rotation_count += h_rot;
+      if (h_rot == 0) break;
+    }
+    if (!tree_levels(N, roots, all_nodes, rot + 1, level_begin, sm))
+      return cuda_fail(ctx, cudaGetLastError(), "BVH levels");
+    // the rotated tree's depth replaces the build's
+    int depth = (int)level_begin.size() - 2;
+    cudaMemcpyAsync(counters + 5, &depth, 4, cudaMemcpyHostToDevice, sm);
+    cudaStreamSynchronize(sm);
+  }
+  rtb_status fs = finish_build(ctx, desc, cfg, W, c, P, I, N, all_nodes, level_begin, roots, total_nodes,
+                               counters, out, stats);
+  if (fs == RTB_OK && stats) stats->rotation_count = rotation_count;
+  return fs;
 }
 
 }  // namespace rtb

@@ -130,6 +130,8 @@ struct Nodes {
   Box* bounds;
   int* size;
   int* pre;
+  int* rsize;   // primitive references under the node
+  int* rfirst;  // the node's first reference in preorder (leaf ranges after rotations)
   double* sah[3];   // generalized, uniform, weighted
 };
 
@@ -188,6 +190,7 @@ __global__ void k_bottom_up(const Prims P, IdxSet I, Nodes N, const int* nodes, 
   int node = nodes[g];
   if (N.leaf[node]) {
     N.size[node] = 1;
+    N.rsize[node] = N.end[node] - N.start[node];
     double c0 = 0.0, c1 = 0.0, c2 = 0.0;
     for (int j = N.start[node]; j < N.end[node]; ++j) {
       int p = current_prim(I.a, N.order_axis[node], j);
@@ -202,6 +205,7 @@ __global__ void k_bottom_up(const Prims P, IdxSet I, Nodes N, const int* nodes, 
   }
   int l = N.left[node], r = N.right[node];
   N.size[node] = 1 + N.size[l] + N.size[r];
+  N.rsize[node] = N.rsize[l] + N.rsize[r];
   double area = surface_area(N.bounds[node]);
   double al = surface_area(N.bounds[l]), ar = surface_area(N.bounds[r]);
   for (int m = 0; m < 3; ++m) {
@@ -224,6 +228,8 @@ __global__ void k_preorder(Nodes N, const int* nodes, int k) {
   if (N.leaf[node]) return;
   int l = N.left[node];
   N.pre[l] = N.pre[node] + 1;
+  N.rfirst[l] = N.rfirst[node];
+  N.rfirst[N.right[node]] = N.rfirst[node] + N.rsize[l];
   N.pre[N.right[node]] = N.pre[node] + 1 + N.size[l];
 }
 
@@ -246,19 +252,20 @@ __global__ void k_flatten(const Prims P, IdxSet I, const Nodes N, int count, flo
     d[3] = 0;
     return;
   }
-  int s = N.start[node], e = N.end[node];
+  // references in preorder of the leaves (after rotations that differs from array order)
+  int s = N.start[node], e = N.end[node], f = N.rfirst[node];
   int t0 = -1;
   bool mixed = false;
   for (int j = s; j < e; ++j) {
     int p = current_prim(I.a, N.order_axis[node], j);
-    refs[j] = P.ref[p];
+    refs[f + (j - s)] = P.ref[p];
     int t = P.type[p];
     if (t0 < 0) t0 = t;
     else if (t != t0) mixed = true;
   }
   d[0] = mixed ? -1 : -2 - t0;
   d[1] = -1;
-  d[2] = s;
+  d[2] = f;
   d[3] = e - s;
 }
 
@@ -288,15 +295,18 @@ struct Workspace {
 // ---- host side shared by the builders
 
 // Validates a build request and fills the per-build constants.
+// allow_rotations: the full-sweep builder also takes the rotation modes (6, 7).
 inline rtb_status build_setup(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_build_config* cfg,
-                              BuildCfg& c, bool& per_type) {
+                              BuildCfg& c, bool& per_type, bool allow_rotations = false) {
   if (!desc || !cfg) return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "null argument");
   if (cfg->mode < 0 || cfg->mode > 7) return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "unknown BVH build mode");
-  if (cfg->mode > 3)
-    return fail(ctx, RTB_ERR_UNSUPPORTED, "SBVH and rotation build modes are not built on the device");
+  if (cfg->mode == 4 || cfg->mode == 5)
+    return fail(ctx, RTB_ERR_UNSUPPORTED, "SBVH build modes are not built on the device");
+  if (cfg->mode > 5 && !allow_rotations)
+    return fail(ctx, RTB_ERR_UNSUPPORTED, "rotation modes apply to the full-sweep builder");
   if (cfg->leaf_size < 1) return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "BVH leaf size must be positive.");
-  bool weighted = cfg->mode == 1 || cfg->mode == 3;
-  per_type = cfg->mode >= 2;
+  bool weighted = cfg->mode == 1 || cfg->mode == 3 || cfg->mode == 7;
+  per_type = cfg->mode == 2 || cfg->mode == 3;
   c.n[0] = desc->sphere_count;
   c.n[1] = desc->box_count;
   c.n[2] = desc->affine_sphere_count;
@@ -369,6 +379,8 @@ inline Nodes alloc_nodes(Workspace& W, int cap) {
   N.bounds = W.alloc<Box>(cap);
   N.size = W.alloc<int>(cap);
   N.pre = W.alloc<int>(cap);
+  N.rsize = W.alloc<int>(cap);
+  N.rfirst = W.alloc<int>(cap);
   for (int m = 0; m < 3; ++m) N.sah[m] = W.alloc<double>(cap);
   return N;
 }
@@ -408,20 +420,23 @@ inline rtb_status finish_build(rtb_context* ctx, const rtb_scene_desc* desc, con
     k_bottom_up<<<blocks(cnt, 128), 128, 0, sm>>>(P, I, N, all_nodes + b, cnt, c.traversal);
   }
   // Tree roots in order: preorder index = sizes of the previous trees.
-  std::vector<int> h_size(roots);
+  std::vector<int> h_size(roots), h_rsize(roots);
   for (int r = 0; r < roots; ++r) cudaMemcpyAsync(&h_size[r], N.size + r, 4, cudaMemcpyDeviceToHost, sm);
+  for (int r = 0; r < roots; ++r) cudaMemcpyAsync(&h_rsize[r], N.rsize + r, 4, cudaMemcpyDeviceToHost, sm);
   double h_sah[4][3];
   for (int r = 0; r < roots; ++r)
     for (int m = 0; m < 3; ++m) cudaMemcpyAsync(&h_sah[r][m], N.sah[m] + r, 8, cudaMemcpyDeviceToHost, sm);
   cudaError_t e = cudaStreamSynchronize(sm);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "BVH sizes");
-  std::vector<int> h_pre(roots);
+  std::vector<int> h_pre(roots), h_rfirst(roots);
   int acc = 0;
   for (int r = 0; r < roots; ++r) {
     h_pre[r] = acc;
     acc += h_size[r];
+    h_rfirst[r] = r ? h_rfirst[r - 1] + h_rsize[r - 1] : 0;
   }
   cudaMemcpyAsync(N.pre, h_pre.data(), roots * 4, cudaMemcpyHostToDevice, sm);
+  cudaMemcpyAsync(N.rfirst, h_rfirst.data(), roots * 4, cudaMemcpyHostToDevice, sm);
   for (int L = 0; L + 1 < (int)level_begin.size(); ++L) {
     int b = level_begin[L], cnt = level_begin[L + 1] - b;
     k_preorder<<<blocks(cnt, 128), 128, 0, sm>>>(N, all_nodes + b, cnt);
@@ -465,6 +480,7 @@ inline rtb_status finish_build(rtb_context* ctx, const rtb_scene_desc* desc, con
     stats->bytes = (long long)total_nodes * 24 + ((long long)total_nodes * 4 + n + roots) * 4;
     stats->build_ms = ms;
     stats->sequential_nodes = 0;
+    stats->rotation_count = 0;
   }
   return RTB_OK;
 }

@@ -91,6 +91,8 @@ rtb_status trace_rays(rtb_context* ctx, rtb_scene* scene, const float* d_rays, i
 // rtb_build.cu
 rtb_status build_bvh(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_build_config* cfg,
                      rtb_scene** out, rtb_bvh_stats* stats);
+rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_build_config* cfg,
+                             const rtb_build_options* options, rtb_scene** out, rtb_bvh_stats* stats);
 
 // rtb_binned.cu
 rtb_status build_bvh_binned(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_build_config* cfg,

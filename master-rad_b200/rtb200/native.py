@@ -54,7 +54,14 @@ class BvhStats(C.Structure):
                 ("min_leaf_occupancy", C.c_int), ("max_leaf_occupancy", C.c_int),
                 ("generalized_sah_cost", C.c_double), ("uniform_sah_cost", C.c_double),
                 ("weighted_sah_cost", C.c_double), ("bytes", C.c_longlong),
-                ("build_ms", C.c_double), ("sequential_nodes", C.c_int)]
+                ("build_ms", C.c_double), ("sequential_nodes", C.c_int),
+                ("rotation_count", C.c_int)]
+
+
+class BuildOptions(C.Structure):
+    _fields_ = [("spatial_bins", C.c_int), ("max_reference_multiplier", C.c_double),
+                ("max_splits_per_primitive", C.c_int), ("min_spatial_references", C.c_int),
+                ("spatial_overlap_threshold", C.c_double), ("rotation_passes", C.c_int)]
 
 
 class Camera(C.Structure):
@@ -119,6 +126,9 @@ SIGNATURES = {
                                    C.POINTER(C.c_void_p)]),
     "rtb_scene_build": (C.c_int, [C.c_void_p, C.POINTER(SceneDesc), C.POINTER(BuildConfig),
                                   C.POINTER(C.c_void_p), C.POINTER(BvhStats)]),
+    "rtb_scene_build_with_options": (C.c_int, [C.c_void_p, C.POINTER(SceneDesc),
+                                               C.POINTER(BuildConfig), C.POINTER(BuildOptions),
+                                               C.POINTER(C.c_void_p), C.POINTER(BvhStats)]),
     "rtb_scene_build_binned": (C.c_int, [C.c_void_p, C.POINTER(SceneDesc), C.POINTER(BuildConfig),
                                          C.c_int, C.POINTER(C.c_void_p), C.POINTER(BvhStats)]),
     "rtb_scene_bvh_sizes": (C.c_int, [C.c_void_p, C.c_void_p, IP, IP, IP]),

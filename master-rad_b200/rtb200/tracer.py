@@ -39,7 +39,7 @@ BvhStats = collections.namedtuple("BvhStats", [
     "node_count", "root_count", "leaf_count", "max_depth", "primitive_ref_count", "leaf_size",
     "build_mode", "generalized_sah_cost", "uniform_sah_cost", "weighted_sah_cost", "bytes",
     "min_leaf_occupancy", "max_leaf_occupancy", "mean_leaf_occupancy", "build_ms",
-    "sequential_nodes"])
+    "sequential_nodes", "rotation_count"])
 
 
 def validate_full_path_depth(max_depth: int) -> None:
@@ -152,14 +152,18 @@ class ResidentScene:
             ctx.check(ctx.lib.rtb_scene_build_binned(ctx.handle, C.byref(d), C.byref(bc), int(bins),
                                                      C.byref(h), C.byref(st)))
         else:
-            ctx.check(ctx.lib.rtb_scene_build(ctx.handle, C.byref(d), C.byref(bc), C.byref(h),
-                                              C.byref(st)))
+            o = scene.options
+            opts = N.BuildOptions(o.spatial_bins, o.max_reference_multiplier,
+                                  o.max_splits_per_primitive, o.min_spatial_references,
+                                  o.spatial_overlap_threshold, o.rotation_passes)
+            ctx.check(ctx.lib.rtb_scene_build_with_options(ctx.handle, C.byref(d), C.byref(bc),
+                                                           C.byref(opts), C.byref(h), C.byref(st)))
         mean = st.primitive_ref_count / st.leaf_count if st.leaf_count else 0.0
         stats = BvhStats(st.node_count, st.root_count, st.leaf_count, st.max_depth,
                          st.primitive_ref_count, st.leaf_size, cfg.mode.name,
                          st.generalized_sah_cost, st.uniform_sah_cost, st.weighted_sah_cost,
                          st.bytes, st.min_leaf_occupancy, st.max_leaf_occupancy, mean,
-                         st.build_ms, st.sequential_nodes)
+                         st.build_ms, st.sequential_nodes, st.rotation_count)
         return ResidentScene(ctx, h, stats)
 
     def download_bvh(self):

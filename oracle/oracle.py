@@ -36,6 +36,7 @@ def lib():
         _lib = C.CDLL(path)
         _lib.orc_build_bvh.restype = C.c_int
         _lib.orc_build_bvh_binned.restype = C.c_int
+        _lib.orc_build_bvh_rotations.restype = C.c_int
         _lib.orc_trace.restype = None
         _lib.orc_render.restype = None
         _lib.orc_cpu_render.restype = C.c_int
@@ -99,9 +100,11 @@ class Bvh:
         return topology_sha256(self.node_bounds, self.node_data, self.refs, self.roots)
 
 
-def build_bvh(scene, config=None, bins=0):
+def build_bvh(scene, config=None, bins=0, rotation_passes=4):
     """Builds the reference BVH for a rtb200.scene.GpuScene (or config override); with
-    bins in 2..32, the library's binned object-SAH mode instead of the full sweep."""
+    bins in 2..32, the library's binned object-SAH mode instead of the full sweep.  The
+    rotation modes apply BvhRotator with ``rotation_passes`` passes; the Bvh's
+    ``rotations`` is the number of rotations made."""
     cfg = config if config is not None else scene.config
     c = _Cfg(int(cfg.mode), cfg.leaf_size, cfg.traversal_weight, cfg.sphere_weight,
              cfg.box_weight, cfg.affine_sphere_weight, cfg.affine_box_weight, cfg.lam)
@@ -118,17 +121,23 @@ def build_bvh(scene, config=None, bins=0):
     sah = np.zeros(3, np.float64)
     outs = (_fp(nbounds), _ip(ndata), _ip(refs), _ip(roots), _ip(counts),
             sah.ctypes.data_as(C.POINTER(C.c_double)))
+    rot = C.c_int(0)
     if bins:
         rc = lib().orc_build_bvh_binned(_fp(sp), ns, _fp(bx), nb, _fp(ab), nas, _fp(bb), nab,
                                         C.byref(c), int(bins), *outs)
+    elif int(cfg.mode) in (6, 7):
+        rc = lib().orc_build_bvh_rotations(_fp(sp), ns, _fp(bx), nb, _fp(ab), nas, _fp(bb), nab,
+                                           C.byref(c), int(rotation_passes), *outs, C.byref(rot))
     else:
         rc = lib().orc_build_bvh(_fp(sp), ns, _fp(bx), nb, _fp(ab), nas, _fp(bb), nab,
                                  C.byref(c), *outs)
     if rc != 0:
         raise RuntimeError("oracle BVH build failed: %d" % rc)
     nn, nr, nref = int(counts[0]), int(counts[1]), int(counts[4])
-    return Bvh(nbounds[:6 * nn].copy(), ndata[:4 * nn].copy(), refs[:nref].copy(),
-               roots[:nr].copy(), counts, sah)
+    out = Bvh(nbounds[:6 * nn].copy(), ndata[:4 * nn].copy(), refs[:nref].copy(),
+              roots[:nr].copy(), counts, sah)
+    out.rotations = rot.value
+    return out
 
 
 def topology_sha256(node_bounds, node_data, refs, roots):

@@ -18,6 +18,11 @@
 //   * per-type forest       gfxlab/gpu/GpuScene.java:702-720
 //   * flattenBvh / leafKind gfxlab/gpu/GpuScene.java:772-808   (preorder)
 //   * SAH statistics        gfxlab/gpu/GpuScene.java:810-838
+//   * BvhRotator            gfxlab/gpu/GpuScene.java:968-1057  (Kensler-style local
+//                           rotations after the SAH build, for the *_ROTATIONS modes:
+//                           bottom-up, four candidates per node, recursive areaCost,
+//                           strict improvement by more than 1e-12, up to rotationPasses
+//                           passes while any rotation happened)
 // Arithmetic is IEEE double with no contraction (Java strictfp semantics); this file
 // must be compiled with -ffp-contract=off.
 //
@@ -356,6 +361,87 @@ struct Builder {
   }
 };
 
+// BvhRotator (GpuScene.java:968-1057) over a Builder's node pool.
+struct Rotator {
+  Builder& b;
+  explicit Rotator(Builder& bb) : b(bb) {}
+
+  int join(int l, int r) {
+    Node n;
+    n.bounds = unite(b.pool[l].bounds, b.pool[r].bounds);
+    n.left = l;
+    n.right = r;
+    b.pool.push_back(n);
+    return (int)b.pool.size() - 1;
+  }
+
+  // areaCost: recursive over the candidate's subtree
+  double area_cost(int n) {
+    const Node nd = b.pool[n];
+    if (nd.left < 0) {
+      double w = 0.0;
+      for (int i = nd.start; i < nd.end; ++i) w += b.objective(b.prims[i]);
+      return surface_area(nd.bounds) * w;
+    }
+    double x = surface_area(nd.bounds) * b.cfg.traversal;
+    x = x + area_cost(nd.left);
+    return x + area_cost(nd.right);
+  }
+
+  // optimizePass: returns the (possibly new) root of the subtree; counts rotations
+  int pass(int n, int& rotations) {
+    if (b.pool[n].left < 0) return n;
+    int l = pass(b.pool[n].left, rotations);
+    int r = pass(b.pool[n].right, rotations);
+    int current = join(l, r);
+    int best = current;
+    double best_cost = area_cost(current);
+    const double eps = 1.0e-12;
+    if (b.pool[b.pool[current].left].left >= 0) {
+      int L = b.pool[current].left;
+      int a = b.pool[L].left, bb = b.pool[L].right, c = b.pool[current].right;
+      int cand = join(a, join(bb, c));
+      double cost = area_cost(cand);
+      if (cost < best_cost - eps) {
+        best = cand;
+        best_cost = cost;
+      }
+      cand = join(bb, join(a, c));
+      cost = area_cost(cand);
+      if (cost < best_cost - eps) {
+        best = cand;
+        best_cost = cost;
+      }
+    }
+    if (b.pool[b.pool[current].right].left >= 0) {
+      int R = b.pool[current].right;
+      int a = b.pool[current].left, bb = b.pool[R].left, c = b.pool[R].right;
+      int cand = join(join(a, c), bb);
+      double cost = area_cost(cand);
+      if (cost < best_cost - eps) {
+        best = cand;
+        best_cost = cost;
+      }
+      cand = join(join(a, bb), c);
+      cost = area_cost(cand);
+      if (cost < best_cost - eps) best = cand;
+    }
+    if (best != current) rotations++;
+    return best;
+  }
+
+  int optimize(int root, int passes, int& total) {
+    total = 0;
+    for (int p = 0; p < passes; ++p) {
+      int rot = 0;
+      root = pass(root, rot);
+      total += rot;
+      if (rot == 0) break;
+    }
+    return root;
+  }
+};
+
 struct Summary {
   int nodes = 0, leaves = 0, max_depth = 0, min_leaf = INT32_MAX, max_leaf = 0;
 };
@@ -470,12 +556,16 @@ typedef struct {
 // Returns 0 on success, negative on an unsupported configuration.
 static int build_any(const float* spheres, int ns, const float* boxes, int nb,
                      const float* affine_sphere_bounds, int nas, const float* affine_box_bounds,
-                     int nab, const orc_build_config* cfg, int bins, float* node_bounds,
-                     int* node_data, int* refs, int* roots, int* counts, double* sah) {
-  if (cfg->mode < 0 || cfg->mode > 3 || cfg->leaf_size < 1) return -1;
+                     int nab, const orc_build_config* cfg, int bins, int rotation_passes,
+                     float* node_bounds, int* node_data, int* refs, int* roots, int* counts,
+                     double* sah, int* rotations_out) {
+  bool rotations = cfg->mode == 6 || cfg->mode == 7;
+  if (cfg->mode < 0 || (cfg->mode > 3 && !rotations) || cfg->leaf_size < 1) return -1;
   if (bins != 0 && (bins < 2 || bins > 32)) return -1;
-  bool weighted = cfg->mode == 1 || cfg->mode == 3;
-  bool per_type = cfg->mode >= 2;
+  if (rotations && (bins != 0 || rotation_passes < 1)) return -1;
+  bool weighted = cfg->mode == 1 || cfg->mode == 3 || cfg->mode == 7;
+  bool per_type = cfg->mode == 2 || cfg->mode == 3;
+  if (rotations_out) *rotations_out = 0;
   Config c{weighted ? 1 : 0, cfg->leaf_size, cfg->traversal_weight,
            weighted ? cfg->lambda : 0.0};
   c.bins = bins;
@@ -554,6 +644,12 @@ static int build_any(const float* spheres, int ns, const float* boxes, int nb,
     Builder b(parts[t], c);
     b.pool.reserve(2 * parts[t].size());
     int root = b.build(0, (int)parts[t].size());
+    if (rotations) {
+      Rotator rot(b);
+      int n_rot = 0;
+      root = rot.optimize(root, rotation_passes, n_rot);
+      if (rotations_out) *rotations_out += n_rot;
+    }
     Summary s;
     summarize(b.pool, root, 0, s);
     total_summary.nodes += s.nodes;
@@ -582,7 +678,18 @@ int orc_build_bvh(const float* spheres, int ns, const float* boxes, int nb,
                   int nab, const orc_build_config* cfg, float* node_bounds, int* node_data,
                   int* refs, int* roots, int* counts, double* sah) {
   return build_any(spheres, ns, boxes, nb, affine_sphere_bounds, nas, affine_box_bounds, nab, cfg,
-                   0, node_bounds, node_data, refs, roots, counts, sah);
+                   0, 4, node_bounds, node_data, refs, roots, counts, sah, nullptr);
+}
+
+// The rotation modes (6 SAH_ROTATIONS, 7 WEIGHTED_SAH_ROTATIONS) with an explicit
+// BvhBuildOptions.rotationPasses; *rotations receives the rotation count.
+int orc_build_bvh_rotations(const float* spheres, int ns, const float* boxes, int nb,
+                            const float* affine_sphere_bounds, int nas,
+                            const float* affine_box_bounds, int nab, const orc_build_config* cfg,
+                            int rotation_passes, float* node_bounds, int* node_data, int* refs,
+                            int* roots, int* counts, double* sah, int* rotations) {
+  return build_any(spheres, ns, boxes, nb, affine_sphere_bounds, nas, affine_box_bounds, nab, cfg,
+                   0, rotation_passes, node_bounds, node_data, refs, roots, counts, sah, rotations);
 }
 
 // Binned object-SAH mode with 2..32 bins per axis (see the header of this file).
@@ -593,7 +700,7 @@ int orc_build_bvh_binned(const float* spheres, int ns, const float* boxes, int n
                          int* counts, double* sah) {
   if (bins < 2 || bins > 32) return -1;
   return build_any(spheres, ns, boxes, nb, affine_sphere_bounds, nas, affine_box_bounds, nab, cfg,
-                   bins, node_bounds, node_data, refs, roots, counts, sah);
+                   bins, 4, node_bounds, node_data, refs, roots, counts, sah, nullptr);
 }
 
 }  // extern "C"

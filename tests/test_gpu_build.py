@@ -112,3 +112,29 @@ def test_device_build_one_million_identical(ctx):
     w = synth.scale_workload()
     st = _check_identical(ctx, w.scene, w.scene.config)
     assert st.primitive_ref_count == 1_000_001
+
+
+@pytest.mark.parametrize("mode", [BvhBuildMode.SAH_ROTATIONS, BvhBuildMode.WEIGHTED_SAH_ROTATIONS])
+@pytest.mark.parametrize("n", [7, 300, 5000])
+def test_device_rotation_modes_identical(ctx, mode, n):
+    """BvhRotator (GpuScene.java:968-1057) after the device SAH build: the same rotated tree
+    as the oracle's restatement, node for node, and the same rotation count."""
+    scene = synth.hetero_scene(n, 300 + n, synth.WORKLOAD_IDS["test"], 5)
+    cfg = BvhBuildConfig.weighted(leaf_size=4, mode=mode) if mode.uses_primitive_weights() \
+        else BvhBuildConfig(mode, 4)
+    st = _check_identical(ctx, scene, cfg)
+    assert st.rotation_count == oracle.build_bvh(scene, cfg).rotations
+
+
+def test_device_rotation_passes_option(ctx):
+    from rtb200.scene import BvhBuildOptions
+    w = synth.hetero_workload()
+    cfg = BvhBuildConfig.weighted(leaf_size=4, mode=BvhBuildMode.WEIGHTED_SAH_ROTATIONS)
+    for passes in (1, 2):
+        want = oracle.build_bvh(w.scene, cfg, rotation_passes=passes)
+        w.scene.options = BvhBuildOptions(rotation_passes=passes)
+        rs = ResidentScene.build(ctx, w.scene, cfg)
+        assert oracle.topology_sha256(*rs.download_bvh()) == want.topology_sha256()
+        assert rs.stats.rotation_count == want.rotations
+        rs.close()
+    w.scene.options = BvhBuildOptions()
