@@ -11,6 +11,7 @@ an unavailable device or a failed/aborted kernel raises ``RuntimeError``
 from __future__ import annotations
 
 import collections
+import time
 import ctypes as C
 from typing import Optional
 
@@ -28,6 +29,11 @@ FrameStats = collections.namedtuple("FrameStats", [
     "plane_tests", "affine_sphere_tests", "affine_box_tests", "stack_overflows",
     "max_stack_size", "internal_node_visits", "leaf_node_visits",
     "homogeneous_leaf_node_visits", "mixed_leaf_node_visits"])
+
+# GpuRayTracer.ConditioningStats (GpuRayTracer.java:434-452)
+ConditioningStats = collections.namedtuple("ConditioningStats", [
+    "physical_kernel_launch_count", "upload_nanos", "kernel_nanos",
+    "maximum_physical_kernel_nanos", "total_nanos"])
 
 TraceReplayResult = collections.namedtuple("TraceReplayResult", [
     "stats", "hit_flags", "hit_distances", "hit_primitive_orders", "hit_material_indices",
@@ -222,6 +228,8 @@ class GpuRayTracer:
         self._resident = None
         self._resident_key = None
         self._last_launches = 0
+        self._last_upload_ns = 0
+        self._last_call_ns = 0
 
     # -- availability --
     def _init(self):
@@ -279,7 +287,11 @@ class GpuRayTracer:
         if scene is None or camera is None:
             raise ValueError("GPU scene and camera must not be null")
         ctx = self._require()
+        t0 = time.perf_counter_ns()
+        before = self._resident
         res = self.ensure_scene_resident(scene, bvh)
+        # renderSample's lastUploadNanos: the scene upload this call made, 0 when resident
+        upload_ns = time.perf_counter_ns() - t0 if res is not before else 0
         p = N.RenderParams(self.width, self.height, self.samples_per_frame, int(max_depth),
                            int(frame_index), int(frame_seed) & 0xFFFFFFFFFFFFFFFF,
                            1 if self.bvh_traversal else 0, 1 if self.collect_metrics else 0, 0)
@@ -287,7 +299,40 @@ class GpuRayTracer:
         ctx.check(ctx.lib.rtb_render_sample(ctx.handle, res.handle, C.byref(cam), C.byref(p),
                                             N.fptr(rgb)))
         self._last_launches = 1
+        self._last_upload_ns = upload_ns
+        self._last_call_ns = time.perf_counter_ns() - t0
         return rgb
+
+    # -- steady-state samples (GpuRayTracer.java:434-467) --
+    def condition_steady_state_sample(self, scene: GpuScene, camera: GpuCamera, max_depth: int,
+                                      frame_index: int, frame_seed: int,
+                                      bvh=None) -> ConditioningStats:
+        """Renders one sample into an internal buffer (making the scene resident) and
+        reports its launch count and times, as conditionSteadyStateSample does."""
+        if getattr(self, "_conditioning", None) is None:
+            self._conditioning = np.zeros(self.width * self.height * 3, np.float32)
+        self.render_sample(self._conditioning, scene, camera, max_depth, frame_index, frame_seed, bvh)
+        st = self.last_frame_stats()
+        return ConditioningStats(self._last_launches, st.upload_nanos, st.kernel_nanos,
+                                 st.maximum_physical_kernel_nanos, st.total_nanos)
+
+    def render_steady_state_sample(self, rgb: np.ndarray, scene: GpuScene, camera: GpuCamera,
+                                   max_depth: int, frame_index: int, frame_seed: int,
+                                   bvh=None) -> np.ndarray:
+        """renderSample that must not upload: raises RuntimeError (IllegalStateException)
+        when the scene was not resident already."""
+        out = self.render_sample(rgb, scene, camera, max_depth, frame_index, frame_seed, bvh)
+        if self._last_upload_ns != 0:
+            raise RuntimeError("A steady-state sample uploaded scene data")
+        return out
+
+    def compiled_ptx_sha256(self) -> str:
+        """Identity of the device code (compiledPtxSha256, GpuRayTracer.java:313-315).  The
+        reference hashes the PTX it JIT-compiles; this library ships its sm_100a code
+        precompiled, so the hash is the SHA-256 of the loaded librtb200.so file."""
+        import hashlib
+        with open(N.LIB_PATH, "rb") as f:
+            return hashlib.sha256(f.read()).hexdigest()
 
     # -- traceReplay --
     def trace_replay(self, scene: GpuScene, rays: np.ndarray, ray_count: Optional[int] = None,
@@ -312,6 +357,7 @@ class GpuRayTracer:
                                            1 if collect_metrics else 0, N.iptr(flags),
                                            N.fptr(dist), N.iptr(order), N.iptr(mat), N.fptr(nrm)))
         self._last_launches = 1
+        self._last_call_ns = 0
         return TraceReplayResult(self.last_frame_stats(), flags, dist, order, mat, nrm)
 
     # -- stats --
@@ -320,8 +366,11 @@ class GpuRayTracer:
         st = N.FrameStats()
         ctx.check(ctx.lib.rtb_last_frame_stats(ctx.handle, C.byref(st)))
         c = list(st.counters)
-        return FrameStats(st.total_ns, st.kernel_ns, st.max_physical_kernel_ns, st.copy_ns,
-                          st.upload_ns, c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], c[8],
+        total, upload = st.total_ns, st.upload_ns
+        if self._last_call_ns:  # the last call was render_sample: its own upload and span
+            total, upload = max(total, self._last_call_ns), self._last_upload_ns
+        return FrameStats(total, st.kernel_ns, st.max_physical_kernel_ns, st.copy_ns,
+                          upload, c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], c[8],
                           c[9], c[10], c[11], c[12], c[13])
 
     def last_physical_kernel_launch_count(self) -> int:

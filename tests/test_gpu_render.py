@@ -128,3 +128,22 @@ def test_rmse_vs_fp64_cpu_renderer(name):
           % (name, rmse, floor, rmse / floor, a.mean(), cpu.mean()))
     assert rmse < 1.3 * floor
     assert abs(a.mean() - cpu.mean()) < 0.05 * cpu.mean()
+
+
+def test_steady_state_samples_and_code_identity():
+    """conditionSteadyStateSample / renderSteadyStateSample (GpuRayTracer.java:434-467): the
+    conditioning call uploads the scene and reports it; the steady-state call reuses the
+    resident scene and refuses a frame that had to upload."""
+    w = _small_hetero(32, 24, 2, 3)
+    with GpuRayTracer(w.width, w.height, w.spp) as t:
+        cond = t.condition_steady_state_sample(w.scene, w.camera, w.max_depth, 0, 5)
+        assert cond.upload_nanos > 0 and cond.physical_kernel_launch_count == 1
+        assert cond.kernel_nanos > 0 and cond.total_nanos >= cond.kernel_nanos
+        rgb = np.zeros(w.width * w.height * 3, np.float32)
+        t.render_steady_state_sample(rgb, w.scene, w.camera, w.max_depth, 1, 6)
+        assert t.last_frame_stats().upload_nanos == 0
+        other = _small_hetero(32, 24, 2, 3)
+        with pytest.raises(RuntimeError):
+            t.render_steady_state_sample(rgb, other.scene, w.camera, w.max_depth, 1, 6)
+        h = t.compiled_ptx_sha256()
+        assert len(h) == 64 and h == t.compiled_ptx_sha256()
