@@ -72,33 +72,58 @@ __global__ void k_weights_unit(const Nodes N, const int* key, const int* level_o
 }
 
 // Weighted prefix / suffix sums in the reference's sequential order, one warp per
-// (node, direction): the warp loads 32 weights at a time (coalesced) and every lane runs the
-// same strictly sequential add chain over the shuffled values, lane j keeping the running
-// sum after element j.  The additions happen in exactly the Java loop's order, so every
-// partial sum is bit-identical to it; only the loads are parallel.
-__global__ void k_weights_seq(const double* wpos, const Nodes N, const int* active, int k, double* pw,
-                              double* sw) {
+// (node, axis, direction), all three axes in one launch: the warp loads 32 weights at a
+// time (coalesced, the next chunk prefetched), broadcasts them to every lane with all 32
+// shuffles issued ahead, and every lane then runs the same strictly sequential chain of 32
+// additions, lane j keeping the running sum after element j.  The additions happen in
+// exactly the Java loop's order (0 + w0 = w0 exactly, then one add per element), so every
+// partial sum is bit-identical to it; only the loads and shuffles are parallel.
+struct WeightChains {
+  const double* w[3];  // weights in each axis order
+  double* pw[3];
+  double* sw[3];
+};
+
+__global__ void __launch_bounds__(128) k_weights_seq(const WeightChains C, const Nodes N, const int* active,
+                                                     int k) {
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
-  if (warp >= 2 * k) return;
-  int node = active[warp >> 1];
-  int s = N.start[node], e = N.end[node];
-  if (e - s < 2) return;
+  if (warp >= 6 * k) return;
+  int node = active[warp / 6];
+  int axis = (warp >> 1) % 3;
   bool suffix = warp & 1;
+  int s = N.start[node], e = N.end[node];
   int n = e - s;
+  if (n < 2) return;
+  const double* wp = C.w[axis];
+  double* out = suffix ? C.sw[axis] : C.pw[axis];
   double acc = 0.0;
+  double w = lane < n ? wp[suffix ? e - 1 - lane : s + lane] : 0.0;
   for (int base = 0; base < n; base += 32) {
     int j = base + lane;
     int pos = suffix ? e - 1 - j : s + j;
-    double w = j < n ? wpos[pos] : 0.0;
-    int m = min(32, n - base);
+    int jn = j + 32;
+    double wn = jn < n ? wp[suffix ? e - 1 - jn : s + jn] : 0.0;  // next chunk
     double mine = 0.0;
-    for (int q = 0; q < m; ++q) {
-      double v = __shfl_sync(0xFFFFFFFFu, w, q);
-      acc = (base == 0 && q == 0) ? v : acc + v;
-      if (q == lane) mine = acc;
+    if (n - base >= 32) {
+      double v[32];
+#pragma unroll
+      for (int q = 0; q < 32; ++q) v[q] = __shfl_sync(0xFFFFFFFFu, w, q);
+#pragma unroll
+      for (int q = 0; q < 32; ++q) {
+        acc = acc + v[q];
+        mine = q == lane ? acc : mine;
+      }
+    } else {
+      int m = n - base;
+      for (int q = 0; q < m; ++q) {
+        double v = __shfl_sync(0xFFFFFFFFu, w, q);
+        acc = acc + v;
+        if (q == lane) mine = acc;
+      }
     }
-    if (j < n) (suffix ? sw : pw)[pos] = mine;
+    if (j < n) out[pos] = mine;
+    w = wn;
   }
 }
 
@@ -135,22 +160,58 @@ __device__ __forceinline__ Cand better(Cand a, Cand b) {
   return a;
 }
 
-// First minimum over (axis, position) for each active node; one block per node.
-__global__ void k_argmin(const Nodes N, const int* active, const double* cost0, const double* cost1,
-                         const double* cost2, double* best_cost, long long* best_flat) {
-  int node = active[blockIdx.x];
+// First minimum over (axis, position) for each active node, with a node's positions
+// spread over fixed-size chunks so that the few huge nodes of the top levels use many blocks.  Every chunk reduces its positions
+// (all three axes) to one (cost, flat) candidate; then the node's minimum cost and, among
+// the chunks that reach it, the smallest flat index are taken with atomics.  The minimum
+// of (cost, flat) in lexicographic order does not depend on the reduction order, so the
+// choice is the reference's strict first minimum.
+constexpr int kArgChunk = 4096;
+
+__global__ void k_arg_chunk_counts(const Nodes N, const int* active, int k, int* counts,
+                                   unsigned long long* best_bits, long long* best_flat) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= k) return;
+  int node = active[g];
+  int len = N.end[node] - N.start[node] - 1;  // candidate positions s+1 .. e-1
+  counts[g] = len > kArgChunk ? (len + kArgChunk - 1) / kArgChunk : 1;
+  best_bits[g] = 0x7FF0000000000000ULL;  // +inf
+  best_flat[g] = 0x7FFFFFFFFFFFFFFFLL;
+}
+
+__global__ void __launch_bounds__(256) k_argmin_chunks(const Nodes N, const int* active, int k,
+                                                       const int* chunk_end, const double* cost0,
+                                                       const double* cost1, const double* cost2,
+                                                       double* part_cost, long long* part_flat,
+                                                       int* part_node, unsigned long long* best_bits) {
+  int b = blockIdx.x;
+  // the node whose chunk range [chunk_end[g-1], chunk_end[g]) holds block b
+  int lo = 0, hi = k;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (chunk_end[mid] <= b) lo = mid + 1;
+    else hi = mid;
+  }
+  int g = lo;
+  if (g >= k) {
+    if (threadIdx.x == 0) part_node[b] = -1;
+    return;
+  }
+  int chunk = b - (g ? chunk_end[g - 1] : 0);
+  int node = active[g];
   int s = N.start[node], e = N.end[node];
   int n = e - s;
+  int j0 = s + 1 + chunk * kArgChunk;
+  int j1 = min(e, j0 + kArgChunk);
   Cand m{CUDART_INF, 0x7FFFFFFFFFFFFFFFLL};
   const double* costs[3] = {cost0, cost1, cost2};
-  for (int a = 0; a < 3; ++a) {
-    for (int j = s + 1 + threadIdx.x; j < e; j += blockDim.x) {
+  for (int a = 0; a < 3; ++a)
+    for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
       double c = costs[a][j];
       if (c != CUDART_INF) m = better(m, Cand{c, (long long)a * n + (j - s)});
     }
-  }
-  __shared__ double sc[32];
-  __shared__ long long sf[32];
+  __shared__ double sc[8];
+  __shared__ long long sf[8];
   for (int off = 16; off > 0; off >>= 1) {
     double oc = __shfl_down_sync(0xFFFFFFFFu, m.cost, off);
     long long of = __shfl_down_sync(0xFFFFFFFFu, m.flat, off);
@@ -164,10 +225,22 @@ __global__ void k_argmin(const Nodes N, const int* active, const double* cost0, 
   __syncthreads();
   if (threadIdx.x == 0) {
     Cand r = Cand{sc[0], sf[0]};
-    for (int k = 1; k < (int)(blockDim.x >> 5); ++k) r = better(r, Cand{sc[k], sf[k]});
-    best_cost[blockIdx.x] = r.cost;
-    best_flat[blockIdx.x] = r.flat;
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q) r = better(r, Cand{sc[q], sf[q]});
+    part_cost[b] = r.cost;
+    part_flat[b] = r.flat;
+    part_node[b] = g;
+    // costs are non-negative: their bit patterns order like the values
+    atomicMin(best_bits + g, (unsigned long long)__double_as_longlong(r.cost));
   }
+}
+
+__global__ void k_argmin_flat(int blocks_total, const double* part_cost, const long long* part_flat,
+                              const int* part_node, const double* best_cost, long long* best_flat) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= blocks_total) return;
+  int g = part_node[b];
+  if (g < 0) return;
+  if (part_cost[b] == best_cost[g]) atomicMin(best_flat + g, part_flat[b]);
 }
 
 // Leaf-or-split decision per active node (GpuScene.java:1424-1447).
@@ -424,9 +497,13 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
   Box* pre = W.alloc<Box>(n);
   Box* pre0 = W.alloc<Box>(n);
   Box* suf = W.alloc<Box>(n);
-  double* pw = W.alloc<double>(n);
-  double* wpos = W.alloc<double>(n);
-  double* sw = W.alloc<double>(n);
+  WeightChains chains;
+  for (int a = 0; a < 3; ++a) {
+    chains.w[a] = W.alloc<double>(n);
+    chains.pw[a] = W.alloc<double>(n);
+    chains.sw[a] = c.weighted || a == 0 ? W.alloc<double>(n) : chains.sw[0];
+    if (!c.weighted && a > 0) chains.pw[a] = chains.pw[0];
+  }
   double* cost[3];
   for (int a = 0; a < 3; ++a) cost[a] = W.alloc<double>(n);
   unsigned char* side = W.alloc<unsigned char>(n);
@@ -442,13 +519,19 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
   int* all_nodes = W.alloc<int>(cap);
   double* best_cost = W.alloc<double>(cap);
   long long* best_flat = W.alloc<long long>(cap);
+  int* arg_counts = W.alloc<int>(cap);
+  int* arg_ends = W.alloc<int>(cap);
+  long long max_arg_blocks = n / kArgChunk + cap;
+  double* part_cost = W.alloc<double>(max_arg_blocks);
+  long long* part_flat = W.alloc<long long>(max_arg_blocks);
+  int* part_node = W.alloc<int>(max_arg_blocks);
   int* counters = W.alloc<int>(8);  // node counter, next count, stats[4]
   int* root_start = W.alloc<int>(4);
   int* root_end = W.alloc<int>(4);
   size_t tmp_bytes = 0, b1 = 0, b2 = 0, b3 = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, b1, skeys, skeys2, svals, svals, n);
   cub::DeviceScan::InclusiveScanByKey(nullptr, b2, key, boxes, pre, BoxUnion(), n);
-  cub::DeviceScan::ExclusiveSum(nullptr, b3, flags, lscan, n);
+  cub::DeviceScan::ExclusiveSum(nullptr, b3, flags, lscan, std::max(n, cap));
   tmp_bytes = std::max(b1, std::max(b2, b3));
   size_t b4 = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, b4, tkeys, tkeys2, svals, svals, n, 0, 2);
@@ -495,6 +578,14 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
   int k = roots, level = 0, total_nodes = roots;
   while (k > 0) {
     level_begin.push_back(level_begin.back() + k);
+    // weight sums of all three axis orders first (one launch for the sequential chains)
+    if (c.weighted) {
+      for (int a = 0; a < 3; ++a)
+        k_gather_weights<<<blocks(n), 256, 0, sm>>>(P, I.a[a], n, const_cast<double*>(chains.w[a]));
+      k_weights_seq<<<blocks(6LL * 32 * k, 128), 128, 0, sm>>>(chains, N, active, k);
+    } else {
+      k_weights_unit<<<blocks(n), 256, 0, sm>>>(N, key, level_of, level, n, chains.pw[0], chains.sw[0]);
+    }
     for (int a = 0; a < 3; ++a) {
       size_t tb = tmp_bytes;
       k_gather_boxes<<<blocks(n), 256, 0, sm>>>(P, I.a[a], n, false, key, boxes, key_rev);
@@ -504,16 +595,23 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
       tb = tmp_bytes;
       cub::DeviceScan::InclusiveScanByKey(tmp, tb, key_rev, boxes, suf, BoxUnion(), n,
                                           cub::Equality(), sm);
-      if (c.weighted) {
-        k_gather_weights<<<blocks(n), 256, 0, sm>>>(P, I.a[a], n, wpos);
-        k_weights_seq<<<blocks(64LL * k, 128), 128, 0, sm>>>(wpos, N, active, k, pw, sw);
-      } else {
-        k_weights_unit<<<blocks(n), 256, 0, sm>>>(N, key, level_of, level, n, pw, sw);
-      }
       k_costs<<<blocks(n), 256, 0, sm>>>(P, I.a[a], N, key, level_of, level, a, n,
-                                         a == 0 ? pre0 : pre, suf, pw, sw, c.traversal, cost[a]);
+                                         a == 0 ? pre0 : pre, suf, chains.pw[a], chains.sw[a],
+                                         c.traversal, cost[a]);
     }
-    k_argmin<<<k, 256, 0, sm>>>(N, active, cost[0], cost[1], cost[2], best_cost, best_flat);
+    {
+      k_arg_chunk_counts<<<blocks(k), 256, 0, sm>>>(N, active, k, arg_counts,
+                                                    (unsigned long long*)best_cost, best_flat);
+      size_t tb = tmp_bytes;
+      cub::DeviceScan::InclusiveSum(tmp, tb, arg_counts, arg_ends, k, sm);
+      // chunks <= (positions / kArgChunk) + one per node; surplus blocks find no node
+      long long nb = (long long)n / kArgChunk + k + 1;
+      k_argmin_chunks<<<(unsigned)nb, 256, 0, sm>>>(N, active, k, arg_ends, cost[0], cost[1], cost[2],
+                                                    part_cost, part_flat, part_node,
+                                                    (unsigned long long*)best_cost);
+      k_argmin_flat<<<blocks(nb), 256, 0, sm>>>((int)nb, part_cost, part_flat, part_node, best_cost,
+                                                best_flat);
+    }
     cudaMemsetAsync(counters + 1, 0, 4, sm);
     k_decide<<<blocks(k), 256, 0, sm>>>(P, I, N, active, k, best_cost, best_flat, pre0, c.leaf_size,
                                         counters, next_active, counters + 1, level_of, level,
