@@ -255,10 +255,18 @@ __device__ __forceinline__ float3 linear9(const float* m, float3 v) {  // K:303-
 
 // traceAffineSphere, K:401-461 (normalizedDirection K:317-336 for degenerate local rays).
 template <bool NORMAL>
+__device__ __forceinline__ float affine_sphere_local(const AffineRay& ar, const float* nm, float3* n);
+
+template <bool NORMAL>
 __device__ __forceinline__ float affine_sphere_test(float4 r0, float4 r1, float4 r2, float3 o,
                                                     float3 d, float dd, const float* nm,
                                                     float3* n) {
-  AffineRay ar = affine_ray(r0, r1, r2, o, d, dd);
+  return affine_sphere_local<NORMAL>(affine_ray(r0, r1, r2, o, d, dd), nm, n);
+}
+
+// The unit-sphere part of traceAffineSphere on the mapped ray.
+template <bool NORMAL>
+__device__ __forceinline__ float affine_sphere_local(const AffineRay& ar, const float* nm, float3* n) {
   float after_local = kEps - ar.shift;
   float solve_a = dot(ar.ld, ar.ld);
   float3 sd = ar.ld;
@@ -308,9 +316,17 @@ __device__ __forceinline__ float affine_sphere_test(float4 r0, float4 r1, float4
 
 // traceAffineBox, K:463-586.
 template <bool NORMAL>
+__device__ __forceinline__ float affine_box_local(const AffineRay& ar, const float* nm, float3* n);
+
+template <bool NORMAL>
 __device__ __forceinline__ float affine_box_test(float4 r0, float4 r1, float4 r2, float3 o, float3 d,
                                                  float dd, const float* nm, float3* n) {
-  AffineRay ar = affine_ray(r0, r1, r2, o, d, dd);
+  return affine_box_local<NORMAL>(affine_ray(r0, r1, r2, o, d, dd), nm, n);
+}
+
+// The unit-box part of traceAffineBox on the mapped ray.
+template <bool NORMAL>
+__device__ __forceinline__ float affine_box_local(const AffineRay& ar, const float* nm, float3* n) {
   float after_local = kEps - ar.shift;
   int axis = 0;
   float sign = 0.0f;
@@ -365,12 +381,12 @@ __device__ __forceinline__ void test_ref(const DevScene& S, int type, int idx, f
     t = sphere_test<false>(__ldg(S.spheres + idx), o, d, dd, &dummy);
   } else if (type == kBox) {
     t = box_test<false>(__ldg(S.boxes + 2 * idx), __ldg(S.boxes + 2 * idx + 1), o, d, &dummy);
-  } else if (type == kAffineSphere) {
-    const float4* r = S.aspheres + 3 * idx;
-    t = affine_sphere_test<false>(__ldg(r), __ldg(r + 1), __ldg(r + 2), o, d, dd, nullptr, &dummy);
   } else {
-    const float4* r = S.aboxes + 3 * idx;
-    t = affine_box_test<false>(__ldg(r), __ldg(r + 1), __ldg(r + 2), o, d, dd, nullptr, &dummy);
+    // both affine types share the ray mapping: one code path for the warp's affine lanes
+    const float4* r = (type == kAffineSphere ? S.aspheres : S.aboxes) + 3 * idx;
+    AffineRay ar = affine_ray(__ldg(r), __ldg(r + 1), __ldg(r + 2), o, d, dd);
+    t = type == kAffineSphere ? affine_sphere_local<false>(ar, nullptr, &dummy)
+                              : affine_box_local<false>(ar, nullptr, &dummy);
   }
   if (METRICS) {
     c->prim++;
