@@ -379,14 +379,36 @@ __device__ __forceinline__ void test_ref(const DevScene& S, int type, int idx, f
   float3 dummy;
   if (type == kSphere) {
     t = sphere_test<false>(__ldg(S.spheres + idx), o, d, dd, &dummy);
-  } else if (type == kBox) {
-    t = box_test<false>(__ldg(S.boxes + 2 * idx), __ldg(S.boxes + 2 * idx + 1), o, d, &dummy);
   } else {
-    // both affine types share the ray mapping: one code path for the warp's affine lanes
-    const float4* r = (type == kAffineSphere ? S.aspheres : S.aboxes) + 3 * idx;
-    AffineRay ar = affine_ray(__ldg(r), __ldg(r + 1), __ldg(r + 2), o, d, dd);
-    t = type == kAffineSphere ? affine_sphere_local<false>(ar, nullptr, &dummy)
-                              : affine_box_local<false>(ar, nullptr, &dummy);
+    // boxes and affine boxes share one slab test, both affine types one ray mapping
+    float3 so = o, sd = d, smin, smax;
+    float after = kEps, shift = 0.0f;
+    bool slab = true;
+    if (type == kBox) {
+      float4 lo = __ldg(S.boxes + 2 * idx), hi = __ldg(S.boxes + 2 * idx + 1);
+      smin = v3(lo.x, lo.y, lo.z);
+      smax = v3(hi.x, hi.y, hi.z);
+    } else {
+      const float4* r = (type == kAffineSphere ? S.aspheres : S.aboxes) + 3 * idx;
+      AffineRay ar = affine_ray(__ldg(r), __ldg(r + 1), __ldg(r + 2), o, d, dd);
+      if (type == kAffineSphere) {
+        t = affine_sphere_local<false>(ar, nullptr, &dummy);
+        slab = false;
+      } else {
+        so = ar.lo;
+        sd = ar.ld;
+        smin = v3(-1.0f, -1.0f, -1.0f);
+        smax = v3(1.0f, 1.0f, 1.0f);
+        after = kEps - ar.shift;
+        shift = ar.shift;
+      }
+    }
+    if (slab) {
+      int axis = 0;
+      float sign = 0.0f;
+      float ts = slab_test<false>(so, sd, smin, smax, after, &axis, &sign);
+      t = (type == kBox || ts == CUDART_INF_F) ? ts : shift + ts;
+    }
   }
   if (METRICS) {
     c->prim++;
