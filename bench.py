@@ -57,7 +57,7 @@ FALLBACK_HBM_GBS = 6650.0
 # dram__bytes_read.sum + dram__bytes_write.sum of k_render per sample, from one ncu capture
 # of the same scene at 512x512x8 spp (profiles/k_render_hetero10k_512x512x8spp_full.md);
 # workloads without a capture report null traffic.
-TRAFFIC_BYTES_PER_SAMPLE = {"hetero": (12.07e6 + 42.11e6) / 2097152}
+TRAFFIC_BYTES_PER_SAMPLE = {"hetero": (11.85e6 + 41.48e6) / 2097152}
 
 
 def parse_args(argv=None):
