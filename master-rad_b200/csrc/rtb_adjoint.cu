@@ -44,7 +44,7 @@ __device__ __forceinline__ float luminance(float3 c) {  // K:181-183
 __device__ __forceinline__ float3 reflect_dir(float3 n, float3 i) {  // K:1022-1024
   return sub(mul(n, 2.0f * dot(i, n)), i);
 }
-__device__ __forceinline__ float3 refract_dir(float3 incoming, float3 n, float eta) {  // K:1026-1039
+static __device__ __noinline__ float3 refract_dir(float3 incoming, float3 n, float eta) {  // K:1026-1039
   float3 i = normalize_safe(incoming);
   float c1 = dot(i, n);
   float ri = (c1 >= 0.0f) ? eta : -1.0f / eta;

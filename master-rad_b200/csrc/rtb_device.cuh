@@ -264,6 +264,28 @@ __device__ __forceinline__ float affine_sphere_test(float4 r0, float4 r1, float4
   return affine_sphere_local<NORMAL>(affine_ray(r0, r1, r2, o, d, dd), nm, n);
 }
 
+// normalizedDirection (K:317-336) for a local direction whose squared length is not a
+// positive finite float: the unit direction and the scale back to the mapped parameter.
+// Out of line: rare, and kept out of the leaf test's code.  False when no direction exists.
+static __device__ __noinline__ bool degenerate_local_direction(float3 dir, float3* sd, float* pscale) {
+  float l2 = dot(dir, dir);
+  if (isfinite(l2) && fabsf(l2 - 1.0f) <= 2.0e-6f) {
+    *sd = dir;
+    *pscale = 1.0f;
+    return true;
+  }
+  float scale = fmaxf(fabsf(dir.x), fmaxf(fabsf(dir.y), fabsf(dir.z)));
+  if (!(scale > 0.0f) || !isfinite(scale)) return false;
+  float3 sc = v3(dir.x / scale, dir.y / scale, dir.z / scale);
+  float sl = sqrtf(dot(sc, sc));
+  float dl = scale * sl;
+  float inv = 1.0f / dl;
+  if (!(inv > 0.0f) || !isfinite(inv)) return false;
+  *sd = mul(sc, 1.0f / sl);
+  *pscale = inv;
+  return true;
+}
+
 // The unit-sphere part of traceAffineSphere on the mapped ray.
 template <bool NORMAL>
 __device__ __forceinline__ float affine_sphere_local(const AffineRay& ar, const float* nm, float3* n) {
@@ -272,22 +294,7 @@ __device__ __forceinline__ float affine_sphere_local(const AffineRay& ar, const 
   float3 sd = ar.ld;
   float pscale = 1.0f;
   if (!(solve_a > 0.0f) || !isfinite(solve_a)) {
-    float3 dir = ar.ld;
-    float l2 = dot(dir, dir);
-    if (isfinite(l2) && fabsf(l2 - 1.0f) <= 2.0e-6f) {
-      sd = dir;
-      pscale = 1.0f;
-    } else {
-      float scale = fmaxf(fabsf(dir.x), fmaxf(fabsf(dir.y), fabsf(dir.z)));
-      if (!(scale > 0.0f) || !isfinite(scale)) return CUDART_INF_F;
-      float3 sc = v3(dir.x / scale, dir.y / scale, dir.z / scale);
-      float sl = sqrtf(dot(sc, sc));
-      float dl = scale * sl;
-      float inv = 1.0f / dl;
-      if (!(inv > 0.0f) || !isfinite(inv)) return CUDART_INF_F;
-      sd = mul(sc, 1.0f / sl);
-      pscale = inv;
-    }
+    if (!degenerate_local_direction(ar.ld, &sd, &pscale)) return CUDART_INF_F;
     solve_a = 1.0f;
   }
   float scaled_after = after_local / pscale;
