@@ -607,7 +607,7 @@ def main():
                  "affine_sphere", "affine_box", "overflows", "max_stack", "internal_nodes",
                  "leaves", "homogeneous_leaves", "mixed_leaves"], cnt)},
             "clocks": clock_info,
-            "gpu_launches": args.steps,
+            "gpu_launches": args.steps * fs.physical_launches,
             "device": ctx.device_info().name,
         }
         if cpu is not None:

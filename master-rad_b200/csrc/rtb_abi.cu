@@ -148,6 +148,7 @@ rtb_status rtb_context_destroy(rtb_context* ctx) {
     cudaFree(ctx->d_work);
     cudaFree(ctx->d_abort);
     cudaFree(ctx->d_stage);
+    cudaFree(ctx->d_tail);
     cudaFreeHost(ctx->h_pinned);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -348,7 +349,7 @@ rtb_status rtb_render_sample(rtb_context* ctx, rtb_scene* scene, const rtb_camer
   st.copy_ns = ns_since(tc);
   st.kernel_ns = (long long)(ms * 1e6);
   st.max_physical_kernel_ns = st.kernel_ns;
-  st.physical_launches = 1;
+  st.physical_launches = ctx->render_launches;
   st.upload_ns = 0;
   if (params->collect_metrics) {
     s = read_counters(ctx, st.counters);

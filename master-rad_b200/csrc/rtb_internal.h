@@ -32,6 +32,10 @@ struct rtb_context {
   size_t stage_bytes = 0;
   void* h_pinned = nullptr;
   size_t pinned_bytes = 0;
+  // Per-sample radiance of the frame's last pixels (rendered one sample per lane).
+  float* d_tail = nullptr;
+  size_t tail_bytes = 0;
+  int render_launches = 0;  // kernels the last render_frame launched
 };
 
 struct rtb_scene {

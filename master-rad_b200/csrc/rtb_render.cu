@@ -9,6 +9,12 @@
 // (GpuKernelSources.java:1284-1293), and each sample consumes the reference's random
 // stream (seed K:1231-1254, jitter and camera K:1256-1264, tracePath K:1061-1165), so the
 // image matches the reference's renderKernel bit for bit under the same arithmetic.
+//
+// The frame's last pixels (about two per resident thread, or all of a small frame) are
+// handed out one sample per queue item instead, so the end of the frame does not wait on
+// a few lanes that each still hold a whole pixel.  Those samples' radiance goes to a
+// buffer in item order and k_sum_tail adds each pixel's samples in sample order, the same
+// FP32 additions as the in-register sum.
 #include "rtb_internal.h"
 
 namespace rtb {
@@ -21,7 +27,10 @@ struct RenderArgs {
   unsigned long long frame_seed;
   float* out;
   long long pixels;
-  unsigned long long* queue;       // pixel queue head
+  long long split;                 // pixels [split, pixels) are queued one sample per item
+  long long items;                 // split + (pixels - split) * spp queue items
+  float* tail;                     // RGB of each tail item, item - split order
+  unsigned long long* queue;       // work queue head
   int* abort_flag;                 // host-set abort
   unsigned long long* counters;    // 14 counters (metrics build) + overflow count
 };
@@ -62,6 +71,7 @@ __global__ void __launch_bounds__(128, 8) k_render(RenderArgs a) {
   // Per-lane state.
   long long pixel = -1;
   int x = 0, y = 0, so = 0;
+  int titem = -1;  // tail item of a single-sample lane, -1 while the lane holds a whole pixel
   uint32_t base_seed = 0, rng = 0;
   float3 acc = v3(0, 0, 0), thr = v3(0, 0, 0), rad = v3(0, 0, 0), o = v3(0, 0, 0), d = v3(0, 0, 0);
   int depth = 0;
@@ -76,19 +86,26 @@ __global__ void __launch_bounds__(128, 8) k_render(RenderArgs a) {
       unsigned long long basep = 0;
       int leader = __ffs(need_mask) - 1;
       if (lane == leader) {
-        basep = (*(volatile int*)a.abort_flag) ? (unsigned long long)a.pixels
+        basep = (*(volatile int*)a.abort_flag) ? (unsigned long long)a.items
                                                : atomicAdd(a.queue, (unsigned long long)__popc(need_mask));
       }
       basep = __shfl_sync(0xFFFFFFFFu, basep, leader);
       if (need) {
         long long p = (long long)basep + __popc(need_mask & ((1u << lane) - 1u));
-        if (p >= a.pixels) {
+        if (p >= a.items) {
           done = true;
         } else {
+          if (p < a.split) {
+            so = 0;
+            titem = -1;
+          } else {
+            titem = (int)(p - a.split);
+            so = (int)((unsigned)titem % (unsigned)a.spp);
+            p = a.split + (long long)((unsigned)titem / (unsigned)a.spp);
+          }
           pixel = p;
           x = (int)(p % a.width);
           y = (int)(p / a.width);
-          so = 0;
           base_seed = pixel_base_seed(a.frame_seed, a.frame_index,
                                       (uint32_t)y * (uint32_t)a.width + (uint32_t)x);
         }
@@ -167,7 +184,14 @@ __global__ void __launch_bounds__(128, 8) k_render(RenderArgs a) {
         }
       }
     }
-    if (finished) {
+    if (finished && titem >= 0) {
+      path = false;
+      float* t = a.tail + 3 * (size_t)titem;
+      t[0] = rad.x;
+      t[1] = rad.y;
+      t[2] = rad.z;
+      pixel = -1;
+    } else if (finished) {
       path = false;
       acc = so == 0 ? rad : add(acc, rad);
       so++;
@@ -198,6 +222,23 @@ __global__ void __launch_bounds__(128, 8) k_render(RenderArgs a) {
     atomicAdd(k + 12, c.homo);
     atomicAdd(k + 13, c.mixed);
   }
+}
+
+// One thread per tail pixel: the in-order FP32 sum of its samples, scaled as in k_render.
+// An aborted frame leaves tail pixels unwritten, like the pixels it never fetched.
+__global__ void __launch_bounds__(256) k_sum_tail(const float* __restrict__ tail, float* out,
+                                                 long long split, int tail_pixels, int spp,
+                                                 const int* abort_flag) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= tail_pixels || *(volatile const int*)abort_flag) return;
+  const float* s = tail + 3 * (size_t)q * spp;
+  float3 acc = v3(s[0], s[1], s[2]);
+  for (int i = 1; i < spp; i++) acc = add(acc, v3(s[3 * i], s[3 * i + 1], s[3 * i + 2]));
+  acc = mul(acc, 1.0f / (float)spp);
+  float* o = out + 3 * (split + q);
+  o[0] = acc.x;
+  o[1] = acc.y;
+  o[2] = acc.z;
 }
 
 template <bool METRICS>
@@ -246,6 +287,12 @@ __global__ void __launch_bounds__(256) k_trace(DevScene S, const float* rays, in
 
 int g_render_blocks_per_sm[2] = {0, 0};
 
+#ifndef RTB_TAIL_FACTOR
+#define RTB_TAIL_FACTOR 2.0
+#endif
+// At most 16M tail samples (192 MB of radiance); larger frames split fewer pixels.
+constexpr long long kMaxTailItems = 1LL << 24;
+
 }  // namespace
 
 rtb_status render_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
@@ -283,14 +330,39 @@ rtb_status render_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* ca
                                                   128, 0);
     if (bps < 1) bps = 1;
   }
-  long long want = (a.pixels + 127) / 128;
+  // Tail: about two pixels per resident thread are split into single samples.
+  long long resident = (long long)ctx->sm_count * bps * 128;
+  long long tail_pixels = std::min<long long>(a.pixels, (long long)(RTB_TAIL_FACTOR * resident));
+  tail_pixels = std::min<long long>(tail_pixels, kMaxTailItems / a.spp);
+  size_t tail_bytes = (size_t)tail_pixels * a.spp * 3 * sizeof(float);
+  if (tail_pixels > 0 && tail_bytes > ctx->tail_bytes) {
+    cudaStreamSynchronize(stream);  // the previous frame's sum may still read the buffer
+    cudaFree(ctx->d_tail);
+    ctx->d_tail = nullptr;
+    ctx->tail_bytes = 0;
+    if (cudaMalloc(&ctx->d_tail, tail_bytes) == cudaSuccess) {
+      ctx->tail_bytes = tail_bytes;
+    } else {
+      cudaGetLastError();  // no buffer: every pixel keeps its samples in one lane
+      ctx->d_tail = nullptr;
+      tail_pixels = 0;
+    }
+  }
+  a.split = a.pixels - tail_pixels;
+  a.items = a.split + tail_pixels * a.spp;
+  a.tail = ctx->d_tail;
+  long long want = (a.items + 127) / 128;
   long long grid = std::min<long long>((long long)ctx->sm_count * bps, want);
   if (timed) cudaEventRecord(ctx->ev0, stream);
   if (metrics)
     k_render<true><<<(unsigned)grid, 128, 0, stream>>>(a);
   else
     k_render<false><<<(unsigned)grid, 128, 0, stream>>>(a);
+  if (tail_pixels > 0)
+    k_sum_tail<<<(unsigned)((tail_pixels + 255) / 256), 256, 0, stream>>>(
+        a.tail, a.out, a.split, (int)tail_pixels, a.spp, a.abort_flag);
   if (timed) cudaEventRecord(ctx->ev1, stream);
+  ctx->render_launches = tail_pixels > 0 ? 2 : 1;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "render launch");
   return RTB_OK;

@@ -298,7 +298,9 @@ class GpuRayTracer:
         cam = camera_struct(camera)
         ctx.check(ctx.lib.rtb_render_sample(ctx.handle, res.handle, C.byref(cam), C.byref(p),
                                             N.fptr(rgb)))
-        self._last_launches = 1
+        st = N.FrameStats()
+        ctx.check(ctx.lib.rtb_last_frame_stats(ctx.handle, C.byref(st)))
+        self._last_launches = st.physical_launches  # the frame kernel, plus the tail sum
         self._last_upload_ns = upload_ns
         self._last_call_ns = time.perf_counter_ns() - t0
         return rgb

@@ -60,6 +60,24 @@ def test_render_matches_reference_kernel_without_contraction(wl):
     np.testing.assert_array_equal(dev.view(np.int32), ref.view(np.int32))
 
 
+@pytest.mark.skipif(not oracle.ref_available("nofmad"), reason="reference kernel not built")
+@pytest.mark.parametrize("size", [(1024, 512, 2), (160, 120, 1000), (96, 64, 1)],
+                         ids=["whole-pixel-and-single-sample-lanes", "sample-buffer-cap", "spp1"])
+def test_render_tail_split_matches_reference_kernel(size):
+    """The frame's last pixels run one sample per lane and are summed by a second kernel.
+    1024x512 holds more pixels than two per resident thread, so whole-pixel lanes and
+    single-sample lanes share the frame; 160x120 at 1000 spp exceeds the 16M-sample
+    buffer, so only its last 16,777 pixels are split; spp 1 makes every item a pixel."""
+    w = _small_hetero(*size, depth=4)
+    bvh = oracle.build_bvh(w.scene)
+    with GpuRayTracer(w.width, w.height, w.spp) as t:
+        dev = t.render_sample(None, w.scene, w.camera, w.max_depth, w.frame_index, w.frame_seed,
+                              bvh=bvh).reshape(-1, 3).copy()
+        assert t.last_physical_kernel_launch_count() == 2
+    ref, _ = oracle.ref_render(w, bvh, variant="nofmad")
+    np.testing.assert_array_equal(dev.view(np.int32), ref.view(np.int32))
+
+
 @pytest.mark.skipif(not oracle.ref_available("fmad"), reason="reference kernel not built")
 def test_render_vs_reference_kernel_as_shipped():
     w = _small_hetero(96, 64, 8, 6)
@@ -137,7 +155,8 @@ def test_steady_state_samples_and_code_identity():
     w = _small_hetero(32, 24, 2, 3)
     with GpuRayTracer(w.width, w.height, w.spp) as t:
         cond = t.condition_steady_state_sample(w.scene, w.camera, w.max_depth, 0, 5)
-        assert cond.upload_nanos > 0 and cond.physical_kernel_launch_count == 1
+        # one frame kernel, plus the tail-sum kernel
+        assert cond.upload_nanos > 0 and cond.physical_kernel_launch_count == 2
         assert cond.kernel_nanos > 0 and cond.total_nanos >= cond.kernel_nanos
         rgb = np.zeros(w.width * w.height * 3, np.float32)
         t.render_steady_state_sample(rgb, w.scene, w.camera, w.max_depth, 1, 6)
