@@ -10,6 +10,10 @@
 // running sum (GpuKernelSources.java:1231-1293, tracePath K:1061-1165), so every job's image
 // is bit-identical to its per-scene frame.
 //
+// The batch's last pixels (about two per resident thread) are queued one sample per item,
+// as in the per-scene frame: their radiance goes to the batch's sample buffer and
+// k_sum_batch_tail adds each pixel's samples in sample order, so images stay bit-identical.
+//
 // Launch parameters (threads per block, job order) come from rtb_batch_autotune, which times
 // the candidates on the batch itself.
 #include <algorithm>
@@ -22,6 +26,10 @@ struct rtb_batch {
   std::vector<rtb_batch_job> jobs;  // in the caller's order
   void* d_jobs = nullptr;           // device job table (in the tuned order)
   long long total_pixels = 0;
+  long long total_items = 0;        // whole pixels + single samples of the queue
+  int tail_pixels = 0;              // pixels rendered one sample per item, over all jobs
+  float* d_tail = nullptr;          // their samples' RGB
+  size_t tail_bytes = 0;
   rtb_batch_tuning tuning{};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -39,8 +47,14 @@ struct BatchJob {
   int width, height, spp, max_depth, frame_index;
   unsigned long long frame_seed;
   float* out;
-  long long begin;  // first batch pixel index of this job
+  long long begin;  // first queue item of this job
+  long long split;  // pixels [split, width*height) are queued one sample per item
+  long long tail_off;  // first sample-buffer slot of the job's single-sample items
+  int tail_begin;      // first tail pixel (over all jobs) of this job
 };
+
+// At most 16M single-sample items (192 MB of radiance) per batch.
+constexpr long long kMaxBatchTailItems = 1LL << 24;
 
 __device__ __forceinline__ float luminance(float3 c) {  // K:181-183
   return c.x * 0.212655f + c.y * 0.715158f + c.z * 0.072187f;
@@ -61,7 +75,7 @@ static __device__ __noinline__ float3 refract_dir(float3 incoming, float3 n, flo
 
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_batch(const BatchJob* jobs, int njobs,
-                                                                   long long total,
+                                                                   long long total, float* tail,
                                                                    unsigned long long* queue,
                                                                    const int* abort_flag) {
   __shared__ long long s_begin[kMaxSharedJobs];
@@ -72,6 +86,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_batch(const BatchJo
   int job = 0;
   long long pixel = -1;
   int x = 0, y = 0, so = 0;
+  long long titem = -1;  // sample-buffer slot of a single-sample lane, -1 for a whole pixel
   uint32_t base_seed = 0, rng = 0;
   float3 acc = v3(0, 0, 0), thr = v3(0, 0, 0), rad = v3(0, 0, 0), o = v3(0, 0, 0), d = v3(0, 0, 0);
   int depth = 0;
@@ -101,9 +116,17 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_batch(const BatchJo
           job = lo;
           const BatchJob& J = jobs[job];
           pixel = g - J.begin;
+          if (pixel < J.split) {
+            so = 0;
+            titem = -1;
+          } else {
+            unsigned t = (unsigned)(pixel - J.split);
+            so = (int)(t % (unsigned)J.spp);
+            pixel = J.split + (long long)(t / (unsigned)J.spp);
+            titem = J.tail_off + t;
+          }
           x = (int)(pixel % J.width);
           y = (int)(pixel / J.width);
-          so = 0;
           uint32_t s = hash_u32((uint32_t)(J.frame_seed & 0xFFFFFFFFULL));  // K:1231-1236
           s ^= hash_u32((uint32_t)(J.frame_seed >> 32));
           s ^= hash_u32((uint32_t)J.frame_index);
@@ -186,7 +209,14 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_batch(const BatchJo
         }
       }
     }
-    if (finished) {
+    if (finished && titem >= 0) {
+      path = false;
+      float* t = tail + 3 * titem;
+      t[0] = rad.x;
+      t[1] = rad.y;
+      t[2] = rad.z;
+      pixel = -1;
+    } else if (finished) {
       path = false;
       acc = so == 0 ? rad : add(acc, rad);
       so++;
@@ -202,28 +232,60 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_batch(const BatchJo
   }
 }
 
-int launch_grid(rtb_context* ctx, int threads, long long total) {
+// One thread per tail pixel of the batch: the in-order FP32 sum of its samples, scaled as in
+// k_batch.  An aborted batch leaves its tail pixels unwritten.
+__global__ void __launch_bounds__(256) k_sum_batch_tail(const BatchJob* jobs, int njobs,
+                                                        const float* __restrict__ tail,
+                                                        int tail_pixels, const int* abort_flag) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= tail_pixels || *(volatile const int*)abort_flag) return;
+  int lo = 0, hi = njobs - 1;  // last job with tail_begin <= q
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].tail_begin <= q) lo = mid; else hi = mid - 1;
+  }
+  const BatchJob& J = jobs[lo];
+  long long k = q - J.tail_begin;  // tail pixel within the job
+  const float* s = tail + 3 * (J.tail_off + k * J.spp);
+  float3 acc = v3(s[0], s[1], s[2]);
+  for (int i = 1; i < J.spp; i++) acc = add(acc, v3(s[3 * i], s[3 * i + 1], s[3 * i + 2]));
+  acc = mul(acc, 1.0f / (float)J.spp);
+  float* o = J.out + 3 * (J.split + k);
+  o[0] = acc.x;
+  o[1] = acc.y;
+  o[2] = acc.z;
+}
+
+int blocks_per_sm(int threads) {
   int bps = 1;
   const void* fn = threads == 64 ? (const void*)k_batch<64>
                  : threads == 256 ? (const void*)k_batch<256> : (const void*)k_batch<128>;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, threads, 0);
-  if (bps < 1) bps = 1;
+  return bps < 1 ? 1 : bps;
+}
+
+int launch_grid(rtb_context* ctx, int threads, long long total) {
   long long want = (total + threads - 1) / threads;
-  return (int)std::max<long long>(1, std::min<long long>((long long)ctx->sm_count * bps, want));
+  return (int)std::max<long long>(
+      1, std::min<long long>((long long)ctx->sm_count * blocks_per_sm(threads), want));
 }
 
 rtb_status enqueue(rtb_context* ctx, rtb_batch* B, cudaStream_t sm) {
   int threads = B->tuning.threads_per_block;
-  int grid = launch_grid(ctx, threads, B->total_pixels);
+  int grid = launch_grid(ctx, threads, B->total_items);
   cudaMemsetAsync(ctx->d_work, 0, sizeof(unsigned long long), sm);
   const BatchJob* J = (const BatchJob*)B->d_jobs;
   int n = (int)B->jobs.size();
+  long long total = B->total_items;
   if (threads == 64)
-    k_batch<64><<<grid, 64, 0, sm>>>(J, n, B->total_pixels, ctx->d_work, ctx->d_abort);
+    k_batch<64><<<grid, 64, 0, sm>>>(J, n, total, B->d_tail, ctx->d_work, ctx->d_abort);
   else if (threads == 256)
-    k_batch<256><<<grid, 256, 0, sm>>>(J, n, B->total_pixels, ctx->d_work, ctx->d_abort);
+    k_batch<256><<<grid, 256, 0, sm>>>(J, n, total, B->d_tail, ctx->d_work, ctx->d_abort);
   else
-    k_batch<128><<<grid, 128, 0, sm>>>(J, n, B->total_pixels, ctx->d_work, ctx->d_abort);
+    k_batch<128><<<grid, 128, 0, sm>>>(J, n, total, B->d_tail, ctx->d_work, ctx->d_abort);
+  if (B->tail_pixels > 0)
+    k_sum_batch_tail<<<(B->tail_pixels + 255) / 256, 256, 0, sm>>>(J, n, B->d_tail, B->tail_pixels,
+                                                                     ctx->d_abort);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? RTB_OK : cuda_fail(ctx, e, "batch launch");
 }
@@ -242,8 +304,41 @@ rtb_status upload_jobs(rtb_context* ctx, rtb_batch* B) {
       return ca > cb;
     });
   }
+  // Tail: the last jobs' last pixels, about two per resident thread, as single samples.
+  std::vector<long long> tail(order.size(), 0);
+  {
+    long long want = 2LL * ctx->sm_count * blocks_per_sm(B->tuning.threads_per_block) *
+                     B->tuning.threads_per_block;
+    long long items_left = kMaxBatchTailItems;
+    for (size_t k = order.size(); k-- > 0 && want > 0;) {
+      const rtb_render_params& p = B->jobs[order[k]].params;
+      long long px = (long long)p.width * p.height;
+      long long tp = std::min(std::min(px, want), items_left / p.samples_per_frame);
+      if (tp <= 0) break;
+      tail[k] = tp;
+      want -= tp;
+      items_left -= tp * p.samples_per_frame;
+      if (tp < px) break;
+    }
+  }
+  long long tail_items = 0, tail_pixels = 0;
+  for (size_t k = 0; k < order.size(); ++k)
+    tail_items += tail[k] * B->jobs[order[k]].params.samples_per_frame;
+  for (long long t : tail) tail_pixels += t;
+  // Job tables and the sample buffer change only while no batch kernel runs.
+  cudaDeviceSynchronize();
+  size_t tail_bytes = (size_t)tail_items * 3 * sizeof(float);
+  if (tail_bytes > B->tail_bytes) {
+    cudaFree(B->d_tail);
+    B->d_tail = nullptr;
+    B->tail_bytes = 0;
+    cudaError_t e = cudaMalloc(&B->d_tail, tail_bytes);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "batch sample buffer");
+    B->tail_bytes = tail_bytes;
+  }
   std::vector<BatchJob> h(order.size());
-  long long begin = 0;
+  long long begin = 0, tail_off = 0;
+  int tail_begin = 0;
   for (size_t k = 0; k < order.size(); ++k) {
     const rtb_batch_job& j = B->jobs[order[k]];
     BatchJob& b = h[k];
@@ -261,7 +356,13 @@ rtb_status upload_jobs(rtb_context* ctx, rtb_batch* B) {
     b.frame_seed = j.params.frame_seed;
     b.out = j.rgb_device;
     b.begin = begin;
-    begin += (long long)j.params.width * j.params.height;
+    long long px = (long long)j.params.width * j.params.height;
+    b.split = px - tail[k];
+    b.tail_off = tail_off;
+    b.tail_begin = tail_begin;
+    begin += b.split + tail[k] * b.spp;
+    tail_off += tail[k] * b.spp;
+    tail_begin += (int)tail[k];
   }
   if (!B->d_jobs) {
     cudaError_t e = cudaMalloc(&B->d_jobs, sizeof(BatchJob) * h.size());
@@ -269,7 +370,10 @@ rtb_status upload_jobs(rtb_context* ctx, rtb_batch* B) {
   }
   cudaError_t e = cudaMemcpy(B->d_jobs, h.data(), sizeof(BatchJob) * h.size(), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "batch job table upload");
-  B->total_pixels = begin;
+  B->total_items = begin;
+  B->tail_pixels = (int)tail_pixels;
+  B->total_pixels = 0;
+  for (const rtb_batch_job& j : B->jobs) B->total_pixels += (long long)j.params.width * j.params.height;
   return RTB_OK;
 }
 
@@ -327,6 +431,7 @@ rtb_status rtb_batch_create(rtb_context* ctx, const rtb_batch_job* jobs, int job
   if (s == RTB_OK) s = capture(ctx, B);
   if (s != RTB_OK) {
     cudaFree(B->d_jobs);
+    cudaFree(B->d_tail);
     delete B;
     return s;
   }
@@ -401,6 +506,7 @@ rtb_status rtb_batch_destroy(rtb_context* ctx, rtb_batch* B) {
   if (B->exec) cudaGraphExecDestroy(B->exec);
   if (B->graph) cudaGraphDestroy(B->graph);
   cudaFree(B->d_jobs);
+  cudaFree(B->d_tail);
   delete B;
   return RTB_OK;
 }

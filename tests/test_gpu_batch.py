@@ -63,3 +63,35 @@ def test_batch_matches_per_scene_frames():
             res.close()
     finally:
         ctx.close()
+
+
+def test_batch_tail_spanning_jobs():
+    """A batch larger than two pixels per resident thread: the first job runs whole pixels,
+    the single-sample tail covers the last job and part of the one before it."""
+    torch = pytest.importorskip("torch")
+    ctx = Context(0)
+    try:
+        specs = [(800, 512, 384, 2, 3), (400, 512, 384, 3, 3), (600, 512, 384, 1, 4)]
+        works, outs, jobs = [], [], []
+        for i, (n, wdt, hgt, spp, depth) in enumerate(specs):
+            s = synth.hetero_scene(n, 500 + i, synth.WORKLOAD_IDS["test"], 30 + i)
+            w = synth.Workload("t%d" % i, s, synth.camera_looking_z((0.0, 0.0, -2.9), wdt / hgt),
+                               wdt, hgt, spp, depth, frame_seed=77 + i, frame_index=i)
+            res = ResidentScene.build(ctx, s)
+            out = torch.zeros(wdt * hgt * 3, dtype=torch.float32, device="cuda")
+            works.append((w, res))
+            outs.append(out)
+            jobs.append((res, w.camera, wdt, hgt, spp, depth, w.frame_index, w.frame_seed, out.data_ptr()))
+        for order in (0, 1):
+            b = Batch(ctx, jobs, tuning={"threads_per_block": 128, "job_order": order})
+            b.render()
+            torch.cuda.synchronize()
+            for (w, res), o in zip(works, outs):
+                np.testing.assert_array_equal(o.cpu().numpy().view(np.int32),
+                                              _single(ctx, res, w, torch).view(np.int32))
+                o.zero_()
+            b.close()
+        for _, res in works:
+            res.close()
+    finally:
+        ctx.close()
