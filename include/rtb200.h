@@ -229,13 +229,16 @@ typedef struct {
 } rtb_batch_job;
 
 typedef struct {
-  int threads_per_block;      /* 64, 128 or 256 */
+  int threads_per_block;      /* 64, 128 or 256 (shared-queue kernel) */
   int job_order;              /* 0: as given, 1: most expensive jobs first */
+  int branches;               /* 0: one shared-queue kernel over all jobs; 1..4: each job
+                                 its own persistent frame, the frames spread round-robin
+                                 over this many concurrent graph branches */
 } rtb_batch_tuning;
 
 typedef struct rtb_batch rtb_batch;
 
-/* tuning may be NULL (128 threads, most expensive first). */
+/* tuning may be NULL (per-job frames over 4 branches, most expensive first). */
 RTB_API rtb_status rtb_batch_create(rtb_context* ctx, const rtb_batch_job* jobs, int job_count,
                                     const rtb_batch_tuning* tuning, rtb_batch** out);
 /* Replays the batch's graph on `stream` (NULL: the context stream); returns once queued. */

@@ -14,8 +14,14 @@
 // as in the per-scene frame: their radiance goes to the batch's sample buffer and
 // k_sum_batch_tail adds each pixel's samples in sample order, so images stay bit-identical.
 //
-// Launch parameters (threads per block, job order) come from rtb_batch_autotune, which times
-// the candidates on the batch itself.
+// Frames mode: with the scene read from a job table instead of kernel parameters, the shared
+// queue costs every sample a little; the alternative is each job's own persistent frame
+// (k_render with its single-sample tail), the frames spread over concurrent branches of the
+// same graph so that one frame's last blocks overlap the next frame's first.  Each frame has
+// its own queue head and sample buffer, so its image is exactly its per-scene frame's.
+//
+// Launch parameters (mode, threads per block, job order, branches) come from
+// rtb_batch_autotune, which times the candidates on the batch itself.
 #include <algorithm>
 #include <numeric>
 #include <vector>
@@ -34,6 +40,14 @@ struct rtb_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int device = 0;
+  // frames mode
+  std::vector<rtb::FramePlan*> frames;   // in the tuned order
+  unsigned long long* d_queues = nullptr;  // one queue head per frame
+  size_t queue_count = 0;
+  float* d_frame_tails = nullptr;          // one sample buffer per branch
+  size_t frame_tail_bytes = 0;
+  cudaStream_t branch[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t fork = nullptr, join[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace rtb {
@@ -270,7 +284,31 @@ int launch_grid(rtb_context* ctx, int threads, long long total) {
       1, std::min<long long>((long long)ctx->sm_count * blocks_per_sm(threads), want));
 }
 
+constexpr int kMaxBranches = 4;
+
+// Frames mode: every job's frame, round-robin over the branches, forked from and joined back
+// into `sm` (inside a capture this builds the graph's parallel branches).
+rtb_status enqueue_frames(rtb_context* ctx, rtb_batch* B, cudaStream_t sm) {
+  int n = (int)B->frames.size();
+  int K = std::min(B->tuning.branches, n);
+  cudaMemsetAsync(B->d_queues, 0, sizeof(unsigned long long) * n, sm);
+  if (K <= 1) {
+    for (FramePlan* f : B->frames) launch_frame(f, sm);
+  } else {
+    cudaEventRecord(B->fork, sm);
+    for (int b = 0; b < K; ++b) cudaStreamWaitEvent(B->branch[b], B->fork, 0);
+    for (int i = 0; i < n; ++i) launch_frame(B->frames[i], B->branch[i % K]);
+    for (int b = 0; b < K; ++b) {
+      cudaEventRecord(B->join[b], B->branch[b]);
+      cudaStreamWaitEvent(sm, B->join[b], 0);
+    }
+  }
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? RTB_OK : cuda_fail(ctx, e, "batch frame launches");
+}
+
 rtb_status enqueue(rtb_context* ctx, rtb_batch* B, cudaStream_t sm) {
+  if (B->tuning.branches > 0) return enqueue_frames(ctx, B, sm);
   int threads = B->tuning.threads_per_block;
   int grid = launch_grid(ctx, threads, B->total_items);
   cudaMemsetAsync(ctx->d_work, 0, sizeof(unsigned long long), sm);
@@ -290,6 +328,61 @@ rtb_status enqueue(rtb_context* ctx, rtb_batch* B, cudaStream_t sm) {
   return e == cudaSuccess ? RTB_OK : cuda_fail(ctx, e, "batch launch");
 }
 
+void free_frames(rtb_batch* B) {
+  for (FramePlan* f : B->frames) delete_frame_plan(f);
+  B->frames.clear();
+}
+
+// Frames mode: one planned frame per job in `order`, its queue head, and one sample buffer
+// per branch sized for the largest tail among that branch's frames.
+rtb_status plan_frames(rtb_context* ctx, rtb_batch* B, const std::vector<int>& order) {
+  free_frames(B);
+  int n = (int)order.size();
+  int K = std::max(1, std::min(B->tuning.branches, n));
+  std::vector<size_t> branch_bytes(K, 0);
+  for (int i = 0; i < n; ++i) {
+    const rtb_batch_job& j = B->jobs[order[i]];
+    rtb_render_params p = j.params;
+    p.collect_metrics = 0;
+    FramePlan* f = new_frame_plan();
+    rtb_status s = plan_frame(ctx, j.scene, &j.camera, &p, j.rgb_device, f);
+    if (s != RTB_OK) {
+      delete_frame_plan(f);
+      free_frames(B);
+      return s;
+    }
+    B->frames.push_back(f);
+    branch_bytes[i % K] = std::max(branch_bytes[i % K], rtb::frame_tail_bytes(f));
+  }
+  std::vector<size_t> off(K, 0);
+  size_t total = 0;
+  for (int b = 0; b < K; ++b) {
+    off[b] = total;
+    total += (branch_bytes[b] + 255) & ~(size_t)255;
+  }
+  if (total > B->frame_tail_bytes) {
+    cudaFree(B->d_frame_tails);
+    B->d_frame_tails = nullptr;
+    B->frame_tail_bytes = 0;
+    cudaError_t e = cudaMalloc(&B->d_frame_tails, total);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "batch frame sample buffers");
+    B->frame_tail_bytes = total;
+  }
+  if ((size_t)n > B->queue_count) {
+    cudaFree(B->d_queues);
+    B->d_queues = nullptr;
+    B->queue_count = 0;
+    cudaError_t e = cudaMalloc(&B->d_queues, sizeof(unsigned long long) * n);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "batch frame queues");
+    B->queue_count = n;
+  }
+  for (int i = 0; i < n; ++i) {
+    float* tail = branch_bytes[i % K] ? (float*)((char*)B->d_frame_tails + off[i % K]) : nullptr;
+    bind_frame(B->frames[i], B->d_queues + i, tail, ctx->d_abort, ctx->d_work + 8);
+  }
+  return RTB_OK;
+}
+
 // Job table in the tuned order: order 0 keeps the caller's order, order 1 puts the most
 // expensive jobs (pixels x spp x depth) first so the batch does not end on a large frame.
 rtb_status upload_jobs(rtb_context* ctx, rtb_batch* B) {
@@ -304,6 +397,9 @@ rtb_status upload_jobs(rtb_context* ctx, rtb_batch* B) {
       return ca > cb;
     });
   }
+  // Job tables and sample buffers change only while no batch kernel runs.
+  cudaDeviceSynchronize();
+  if (B->tuning.branches > 0) return plan_frames(ctx, B, order);
   // Tail: the last jobs' last pixels, about two per resident thread, as single samples.
   std::vector<long long> tail(order.size(), 0);
   {
@@ -325,8 +421,6 @@ rtb_status upload_jobs(rtb_context* ctx, rtb_batch* B) {
   for (size_t k = 0; k < order.size(); ++k)
     tail_items += tail[k] * B->jobs[order[k]].params.samples_per_frame;
   for (long long t : tail) tail_pixels += t;
-  // Job tables and the sample buffer change only while no batch kernel runs.
-  cudaDeviceSynchronize();
   size_t tail_bytes = (size_t)tail_items * 3 * sizeof(float);
   if (tail_bytes > B->tail_bytes) {
     cudaFree(B->d_tail);
@@ -377,6 +471,22 @@ rtb_status upload_jobs(rtb_context* ctx, rtb_batch* B) {
   return RTB_OK;
 }
 
+void release_batch(rtb_batch* B) {
+  if (B->exec) cudaGraphExecDestroy(B->exec);
+  if (B->graph) cudaGraphDestroy(B->graph);
+  free_frames(B);
+  cudaFree(B->d_jobs);
+  cudaFree(B->d_tail);
+  cudaFree(B->d_queues);
+  cudaFree(B->d_frame_tails);
+  for (int b = 0; b < kMaxBranches; ++b) {
+    if (B->branch[b]) cudaStreamDestroy(B->branch[b]);
+    if (B->join[b]) cudaEventDestroy(B->join[b]);
+  }
+  if (B->fork) cudaEventDestroy(B->fork);
+  delete B;
+}
+
 rtb_status capture(rtb_context* ctx, rtb_batch* B) {
   if (B->exec) cudaGraphExecDestroy(B->exec);
   if (B->graph) cudaGraphDestroy(B->graph);
@@ -421,18 +531,30 @@ rtb_status rtb_batch_create(rtb_context* ctx, const rtb_batch_job* jobs, int job
   B->jobs.assign(jobs, jobs + job_count);
   B->tuning.threads_per_block = 128;
   B->tuning.job_order = 1;
+  B->tuning.branches = 4;
   if (tuning) B->tuning = *tuning;
   if (B->tuning.threads_per_block != 64 && B->tuning.threads_per_block != 128 &&
       B->tuning.threads_per_block != 256) {
     delete B;
     return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "threads_per_block must be 64, 128 or 256");
   }
+  if (B->tuning.branches < 0 || B->tuning.branches > kMaxBranches) {
+    delete B;
+    return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "branches must be in [0, 4]");
+  }
+  cudaError_t e = cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming);
+  for (int b = 0; b < kMaxBranches && e == cudaSuccess; ++b) {
+    e = cudaStreamCreateWithFlags(&B->branch[b], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&B->join[b], cudaEventDisableTiming);
+  }
+  if (e != cudaSuccess) {
+    release_batch(B);
+    return cuda_fail(ctx, e, "batch streams");
+  }
   rtb_status s = upload_jobs(ctx, B);
   if (s == RTB_OK) s = capture(ctx, B);
   if (s != RTB_OK) {
-    cudaFree(B->d_jobs);
-    cudaFree(B->d_tail);
-    delete B;
+    release_batch(B);
     return s;
   }
   *out = B;
@@ -458,41 +580,50 @@ rtb_status rtb_batch_autotune(rtb_context* ctx, rtb_batch* B, int repeats, rtb_b
   std::lock_guard<std::mutex> lock(ctx->mu);
   cudaSetDevice(ctx->device);
   if (repeats < 1) repeats = 1;
-  const int threads[3] = {64, 128, 256};
+  // Candidates: the shared-queue kernel at 64/128/256 threads, and per-job frames over
+  // 1/2/4 graph branches; each in the caller's order and most expensive first.
+  std::vector<rtb_batch_tuning> cands;
+  for (int order = 0; order < 2; ++order) {
+    for (int t : {64, 128, 256}) cands.push_back({t, order, 0});
+    for (int k : {1, 2, 4}) cands.push_back({128, order, k});
+  }
   double best_time = 1e300;
   rtb_batch_tuning pick = B->tuning;
   cudaStream_t sm = ctx->stream;
   ctx_acquire(ctx, sm);
-  for (int order = 0; order < 2; ++order) {
-    for (int t : threads) {
-      B->tuning.threads_per_block = t;
-      B->tuning.job_order = order;
-      rtb_status s = upload_jobs(ctx, B);
-      if (s != RTB_OK) return s;
-      double total = 0.0;
-      for (int r = 0; r <= repeats; ++r) {  // first run warms up
-        cudaEventRecord(ctx->ev0, sm);
-        s = enqueue(ctx, B, sm);
-        if (s != RTB_OK) return s;
-        cudaEventRecord(ctx->ev1, sm);
-        cudaError_t e = cudaEventSynchronize(ctx->ev1);
-        if (e != cudaSuccess) return cuda_fail(ctx, e, "batch autotune");
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-        if (r > 0) total += ms;
+  rtb_status s = RTB_OK;
+  for (const rtb_batch_tuning& c : cands) {
+    B->tuning = c;
+    s = upload_jobs(ctx, B);
+    if (s != RTB_OK) break;
+    double total = 0.0;
+    for (int r = 0; r <= repeats && s == RTB_OK; ++r) {  // first run warms up
+      cudaEventRecord(ctx->ev0, sm);
+      s = enqueue(ctx, B, sm);
+      if (s != RTB_OK) break;
+      cudaEventRecord(ctx->ev1, sm);
+      cudaError_t e = cudaEventSynchronize(ctx->ev1);
+      if (e != cudaSuccess) {
+        s = cuda_fail(ctx, e, "batch autotune");
+        break;
       }
-      double mean = total / repeats;
-      if (mean < best_time) {
-        best_time = mean;
-        pick = B->tuning;
-      }
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+      if (r > 0) total += ms;
+    }
+    if (s != RTB_OK) break;
+    double mean = total / repeats;
+    if (mean < best_time) {
+      best_time = mean;
+      pick = c;
     }
   }
-  B->tuning = pick;
   ctx_release(ctx, sm);
-  rtb_status s = upload_jobs(ctx, B);
-  if (s == RTB_OK) s = capture(ctx, B);
+  B->tuning = pick;
+  rtb_status s2 = upload_jobs(ctx, B);
+  if (s2 == RTB_OK) s2 = capture(ctx, B);
   if (s != RTB_OK) return s;
+  if (s2 != RTB_OK) return s2;
   if (best) *best = pick;
   if (best_ms) *best_ms = best_time;
   return RTB_OK;
@@ -502,12 +633,8 @@ rtb_status rtb_batch_destroy(rtb_context* ctx, rtb_batch* B) {
   if (!ctx || !B) return RTB_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(ctx->mu);
   cudaSetDevice(ctx->device);
-  cudaStreamSynchronize(ctx->stream);
-  if (B->exec) cudaGraphExecDestroy(B->exec);
-  if (B->graph) cudaGraphDestroy(B->graph);
-  cudaFree(B->d_jobs);
-  cudaFree(B->d_tail);
-  delete B;
+  cudaDeviceSynchronize();
+  release_batch(B);
   return RTB_OK;
 }
 

@@ -85,6 +85,20 @@ void scene_free(rtb_scene* s, cudaStream_t stream);
 rtb_status render_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
                         const rtb_render_params* p, float* d_rgb, cudaStream_t stream,
                         bool timed);
+// One frame's launch, planned apart from where it runs (the batch's frames mode launches
+// many into one graph).  plan_frame validates and sizes; bind_frame gives it a queue head
+// (zeroed before launch), a sample buffer of frame_tail_bytes (nullptr: no single-sample
+// tail), the abort flag and 14 counters; launch_frame enqueues its kernels and returns how
+// many.
+struct FramePlan;
+FramePlan* new_frame_plan();
+void delete_frame_plan(FramePlan* f);
+rtb_status plan_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
+                      const rtb_render_params* p, float* d_rgb, FramePlan* f);
+size_t frame_tail_bytes(const FramePlan* f);
+void bind_frame(FramePlan* f, unsigned long long* queue, float* tail, int* abort_flag,
+                unsigned long long* counters);
+int launch_frame(const FramePlan* f, cudaStream_t stream);
 // Closest-hit launch without a context (no counters, no allocation).
 cudaError_t launch_trace(const DevScene& scene, int use_bvh, const float* d_rays, int n, int* d_flags,
                          float* d_t, int* d_order, int* d_mat, float* d_normal, cudaStream_t stream);

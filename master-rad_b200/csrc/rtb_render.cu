@@ -295,15 +295,50 @@ constexpr long long kMaxTailItems = 1LL << 24;
 
 }  // namespace
 
-rtb_status render_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
-                        const rtb_render_params* p, float* d_rgb, cudaStream_t stream, bool timed) {
+// One frame's launch: arguments, grid, and how many of its last pixels run one sample per
+// item.  Built by plan_frame; the caller binds the queue, sample buffer and flags.
+struct FramePlan {
+  RenderArgs a;
+  int metrics = 0;
+  long long resident = 0;     // threads of a full-occupancy grid
+  long long tail_pixels = 0;  // the frame's last pixels, queued one sample per item
+  long long grid = 0;
+};
+
+namespace {
+
+int frame_blocks_per_sm(int metrics) {
+  int& bps = g_render_blocks_per_sm[metrics];
+  if (bps == 0) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, metrics ? (const void*)k_render<true>
+                                                                : (const void*)k_render<false>,
+                                                  128, 0);
+    if (bps < 1) bps = 1;
+  }
+  return bps;
+}
+
+void set_tail(FramePlan* f, long long tail_pixels) {
+  RenderArgs& a = f->a;
+  f->tail_pixels = tail_pixels;
+  a.split = a.pixels - tail_pixels;
+  a.items = a.split + tail_pixels * a.spp;
+  long long want = (a.items + 127) / 128;
+  f->grid = std::min<long long>(f->resident / 128, want);
+}
+
+}  // namespace
+
+rtb_status plan_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
+                      const rtb_render_params* p, float* d_rgb, FramePlan* f) {
   if (!scene || !cam || !p || !d_rgb) return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "null argument");
   if (p->width < 1 || p->height < 1 || p->samples_per_frame < 1)
     return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "image size and samples must be positive");
   if (p->max_depth < 0 || p->max_depth > 32)
     return fail(ctx, RTB_ERR_INVALID_ARGUMENT,
                 "GPU full-path depth must be in [0, 32] but was " + std::to_string(p->max_depth));
-  RenderArgs a;
+  RenderArgs& a = f->a;
+  a = RenderArgs{};
   a.S = scene->dev;
   a.S.use_bvh = (p->use_bvh && scene->has_bvh) ? 1 : 0;
   a.cam_pos = make_float3(cam->position[0], cam->position[1], cam->position[2]);
@@ -318,24 +353,49 @@ rtb_status render_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* ca
   a.frame_seed = p->frame_seed;
   a.out = d_rgb;
   a.pixels = (long long)p->width * p->height;
-  a.queue = ctx->d_work;
-  a.abort_flag = ctx->d_abort;
-  a.counters = ctx->d_work + 8;
-  cudaMemsetAsync(ctx->d_work, 0, 32 * sizeof(unsigned long long), stream);
-  int metrics = p->collect_metrics ? 1 : 0;
-  int& bps = g_render_blocks_per_sm[metrics];
-  if (bps == 0) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, metrics ? (const void*)k_render<true>
-                                                                : (const void*)k_render<false>,
-                                                  128, 0);
-    if (bps < 1) bps = 1;
-  }
+  f->metrics = p->collect_metrics ? 1 : 0;
+  f->resident = (long long)ctx->sm_count * frame_blocks_per_sm(f->metrics) * 128;
   // Tail: about two pixels per resident thread are split into single samples.
-  long long resident = (long long)ctx->sm_count * bps * 128;
-  long long tail_pixels = std::min<long long>(a.pixels, (long long)(RTB_TAIL_FACTOR * resident));
-  tail_pixels = std::min<long long>(tail_pixels, kMaxTailItems / a.spp);
-  size_t tail_bytes = (size_t)tail_pixels * a.spp * 3 * sizeof(float);
-  if (tail_pixels > 0 && tail_bytes > ctx->tail_bytes) {
+  long long tail_pixels = std::min<long long>(a.pixels, (long long)(RTB_TAIL_FACTOR * f->resident));
+  set_tail(f, std::min<long long>(tail_pixels, kMaxTailItems / a.spp));
+  return RTB_OK;
+}
+
+size_t frame_tail_bytes(const FramePlan* f) {
+  return (size_t)f->tail_pixels * f->a.spp * 3 * sizeof(float);
+}
+
+void bind_frame(FramePlan* f, unsigned long long* queue, float* tail, int* abort_flag,
+                unsigned long long* counters) {
+  if (!tail) set_tail(f, 0);  // no buffer: every pixel keeps its samples in one lane
+  f->a.queue = queue;
+  f->a.tail = tail;
+  f->a.abort_flag = abort_flag;
+  f->a.counters = counters;
+}
+
+int launch_frame(const FramePlan* f, cudaStream_t stream) {
+  const RenderArgs& a = f->a;
+  if (f->metrics)
+    k_render<true><<<(unsigned)f->grid, 128, 0, stream>>>(a);
+  else
+    k_render<false><<<(unsigned)f->grid, 128, 0, stream>>>(a);
+  if (f->tail_pixels == 0) return 1;
+  k_sum_tail<<<(unsigned)((f->tail_pixels + 255) / 256), 256, 0, stream>>>(
+      a.tail, a.out, a.split, (int)f->tail_pixels, a.spp, a.abort_flag);
+  return 2;
+}
+
+FramePlan* new_frame_plan() { return new FramePlan(); }
+void delete_frame_plan(FramePlan* f) { delete f; }
+
+rtb_status render_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
+                        const rtb_render_params* p, float* d_rgb, cudaStream_t stream, bool timed) {
+  FramePlan f;
+  rtb_status s = plan_frame(ctx, scene, cam, p, d_rgb, &f);
+  if (s != RTB_OK) return s;
+  size_t tail_bytes = frame_tail_bytes(&f);
+  if (tail_bytes > ctx->tail_bytes) {
     cudaStreamSynchronize(stream);  // the previous frame's sum may still read the buffer
     cudaFree(ctx->d_tail);
     ctx->d_tail = nullptr;
@@ -343,26 +403,15 @@ rtb_status render_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* ca
     if (cudaMalloc(&ctx->d_tail, tail_bytes) == cudaSuccess) {
       ctx->tail_bytes = tail_bytes;
     } else {
-      cudaGetLastError();  // no buffer: every pixel keeps its samples in one lane
+      cudaGetLastError();
       ctx->d_tail = nullptr;
-      tail_pixels = 0;
     }
   }
-  a.split = a.pixels - tail_pixels;
-  a.items = a.split + tail_pixels * a.spp;
-  a.tail = ctx->d_tail;
-  long long want = (a.items + 127) / 128;
-  long long grid = std::min<long long>((long long)ctx->sm_count * bps, want);
+  bind_frame(&f, ctx->d_work, ctx->d_tail, ctx->d_abort, ctx->d_work + 8);
+  cudaMemsetAsync(ctx->d_work, 0, 32 * sizeof(unsigned long long), stream);
   if (timed) cudaEventRecord(ctx->ev0, stream);
-  if (metrics)
-    k_render<true><<<(unsigned)grid, 128, 0, stream>>>(a);
-  else
-    k_render<false><<<(unsigned)grid, 128, 0, stream>>>(a);
-  if (tail_pixels > 0)
-    k_sum_tail<<<(unsigned)((tail_pixels + 255) / 256), 256, 0, stream>>>(
-        a.tail, a.out, a.split, (int)tail_pixels, a.spp, a.abort_flag);
+  ctx->render_launches = launch_frame(&f, stream);
   if (timed) cudaEventRecord(ctx->ev1, stream);
-  ctx->render_launches = tail_pixels > 0 ? 2 : 1;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "render launch");
   return RTB_OK;

@@ -30,7 +30,8 @@ class Batch:
         self._jobs = arr
         t = None
         if tuning is not None:
-            t = N.BatchTuning(int(tuning["threads_per_block"]), int(tuning["job_order"]))
+            t = N.BatchTuning(int(tuning["threads_per_block"]), int(tuning["job_order"]),
+                              int(tuning.get("branches", 0)))
         h = C.c_void_p()
         ctx.check(ctx.lib.rtb_batch_create(ctx.handle, arr, len(jobs), C.byref(t) if t else None,
                                            C.byref(h)))
@@ -46,7 +47,7 @@ class Batch:
         self.ctx.check(self.ctx.lib.rtb_batch_autotune(self.ctx.handle, self.handle, repeats,
                                                        C.byref(best), C.byref(ms)))
         return {"threads_per_block": best.threads_per_block, "job_order": best.job_order,
-                "ms": ms.value}
+                "branches": best.branches, "ms": ms.value}
 
     def close(self):
         if self.handle:

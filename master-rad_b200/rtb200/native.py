@@ -112,7 +112,7 @@ class CalibrationResult(C.Structure):
 
 
 class BatchTuning(C.Structure):
-    _fields_ = [("threads_per_block", C.c_int), ("job_order", C.c_int)]
+    _fields_ = [("threads_per_block", C.c_int), ("job_order", C.c_int), ("branches", C.c_int)]
 
 
 # Every symbol include/rtb200.h declares, with its ctypes signature.

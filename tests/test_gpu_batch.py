@@ -51,6 +51,7 @@ def test_batch_matches_per_scene_frames():
                                               _single(ctx, res, w, torch).view(np.int32))
         best = b.autotune(repeats=1)
         assert best["threads_per_block"] in (64, 128, 256) and best["job_order"] in (0, 1)
+        assert best["branches"] in (0, 1, 2, 4)
         for o in outs:
             o.zero_()
         b.render()
@@ -66,8 +67,10 @@ def test_batch_matches_per_scene_frames():
 
 
 def test_batch_tail_spanning_jobs():
-    """A batch larger than two pixels per resident thread: the first job runs whole pixels,
-    the single-sample tail covers the last job and part of the one before it."""
+    """A batch larger than two pixels per resident thread: in the shared-queue kernel the
+    first job runs whole pixels and the single-sample tail covers the last job and part of
+    the one before it; in frames mode (1, 2 or 4 graph branches) each job is its own frame
+    with its own queue and sample buffer."""
     torch = pytest.importorskip("torch")
     ctx = Context(0)
     try:
@@ -82,8 +85,10 @@ def test_batch_tail_spanning_jobs():
             works.append((w, res))
             outs.append(out)
             jobs.append((res, w.camera, wdt, hgt, spp, depth, w.frame_index, w.frame_seed, out.data_ptr()))
-        for order in (0, 1):
-            b = Batch(ctx, jobs, tuning={"threads_per_block": 128, "job_order": order})
+        tunings = [{"threads_per_block": 128, "job_order": o, "branches": k}
+                   for o in (0, 1) for k in (0, 1, 2, 4)]
+        for tuning in tunings:
+            b = Batch(ctx, jobs, tuning=tuning)
             b.render()
             torch.cuda.synchronize()
             for (w, res), o in zip(works, outs):
