@@ -467,7 +467,9 @@ __device__ __noinline__ void test_all_primitives(const DevScene& S, float3 o, fl
 // active = false).  The traversal loop is warp-uniform -- each iteration every lane that
 // still has work processes one node: it tests both child boxes, then tests the primitives
 // of the (at most two) leaf children in one loop, then picks the next interior node -- and
-// the loop condition is a warp vote, so divergent lanes reconverge once per node.
+// the loop condition is a warp vote, so divergent lanes reconverge once per node.  Every lane
+// takes part in the votes, also where lanes hold different scenes and only some of them
+// have a tree (the batch kernel's lanes may belong to different jobs).
 template <bool METRICS>
 __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active, Best& b,
                               TraceCounters* c, int* overflow_flag) {
@@ -476,13 +478,14 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
   b.type = -1;
   b.index = -1;
   float dd = dot(d, d);
-  if (S.use_bvh && S.node_count > 0) {
+  const bool bvh = S.use_bvh && S.node_count > 0;
+  {
     float3 inv = v3(d.x != 0.0f ? 1.0f / d.x : 1e30f, d.y != 0.0f ? 1.0f / d.y : 1e30f,
                     d.z != 0.0f ? 1.0f / d.z : 1e30f);
     int stack[kStackSize];
     float estack[kStackSize];
     int sp = 0;
-    int node = active ? 0 : -1;
+    int node = (active && bvh) ? 0 : -1;
     bool overflow = false;
     // A tree visits each node at most once per ray; the cap only matters for malformed
     // (cyclic) caller-supplied trees, which then take the exhaustive path.
@@ -555,9 +558,8 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
       if (METRICS) c->overflow++;
       test_all_refs<METRICS>(S, o, d, dd, b, c);
     }
-  } else if (active) {
-    test_all_primitives<METRICS>(S, o, d, dd, b, c);
   }
+  if (active && !bvh) test_all_primitives<METRICS>(S, o, d, dd, b, c);
   if (!active) return false;
   // tracePlane, K:708-734: a plane wins only when strictly closer.
   for (int i = 0; i < S.plane_count; ++i) {

@@ -290,8 +290,9 @@ int g_render_blocks_per_sm[2] = {0, 0};
 #ifndef RTB_TAIL_FACTOR
 #define RTB_TAIL_FACTOR 2.0
 #endif
-// At most 16M tail samples (192 MB of radiance); larger frames split fewer pixels.
-constexpr long long kMaxTailItems = 1LL << 24;
+// At most 64M tail samples (768 MB of radiance, held by the context); frames whose last
+// two pixels per resident thread hold more samples split fewer pixels.
+constexpr long long kMaxTailItems = 1LL << 26;
 
 }  // namespace
 

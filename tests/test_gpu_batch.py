@@ -100,3 +100,35 @@ def test_batch_tail_spanning_jobs():
             res.close()
     finally:
         ctx.close()
+
+
+def test_batch_mixes_tree_and_linear_scenes():
+    """The shared-queue kernel with a scene that has a tree beside one that has none (tested
+    primitive by primitive): warps at the boundary hold lanes of both, and every image still
+    equals its own frame."""
+    torch = pytest.importorskip("torch")
+    ctx = Context(0)
+    try:
+        works, outs, jobs, scenes = [], [], [], []
+        for i, (n, tree) in enumerate([(300, True), (120, False), (500, True)]):
+            s = synth.hetero_scene(n, 700 + i, synth.WORKLOAD_IDS["test"], 40 + i)
+            w = synth.Workload("m%d" % i, s, synth.camera_looking_z((0.0, 0.0, -2.9), 40 / 30),
+                               40, 30, 3, 4, frame_seed=300 + i, frame_index=i)
+            res = ResidentScene.build(ctx, s) if tree else ResidentScene.upload(ctx, s, None)
+            out = torch.zeros(40 * 30 * 3, dtype=torch.float32, device="cuda")
+            works.append((w, res))
+            outs.append(out)
+            jobs.append((res, w.camera, 40, 30, 3, 4, w.frame_index, w.frame_seed, out.data_ptr()))
+        for threads in (64, 128, 256):
+            b = Batch(ctx, jobs, tuning={"threads_per_block": threads, "job_order": 0, "branches": 0})
+            b.render()
+            torch.cuda.synchronize()
+            for (w, res), o in zip(works, outs):
+                np.testing.assert_array_equal(o.cpu().numpy().view(np.int32),
+                                              _single(ctx, res, w, torch).view(np.int32))
+                o.zero_()
+            b.close()
+        for _, res in works:
+            res.close()
+    finally:
+        ctx.close()
