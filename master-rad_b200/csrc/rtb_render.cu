@@ -10,7 +10,7 @@
 // stream (seed K:1231-1254, jitter and camera K:1256-1264, tracePath K:1061-1165), so the
 // image matches the reference's renderKernel bit for bit under the same arithmetic.
 //
-// The frame's last pixels (about two per resident thread, or all of a small frame) are
+// The frame's last pixels (about four per resident thread, or all of a small frame) are
 // handed out one sample per queue item instead, so the end of the frame does not wait on
 // a few lanes that each still hold a whole pixel.  Those samples' radiance goes to a
 // buffer in item order and k_sum_tail adds each pixel's samples in sample order, the same
@@ -288,10 +288,10 @@ __global__ void __launch_bounds__(256) k_trace(DevScene S, const float* rays, in
 int g_render_blocks_per_sm[2] = {0, 0};
 
 #ifndef RTB_TAIL_FACTOR
-#define RTB_TAIL_FACTOR 2.0
+#define RTB_TAIL_FACTOR 4.0
 #endif
 // At most 64M tail samples (768 MB of radiance, held by the context); frames whose last
-// two pixels per resident thread hold more samples split fewer pixels.
+// four pixels per resident thread hold more samples split fewer pixels.
 constexpr long long kMaxTailItems = 1LL << 26;
 
 }  // namespace
@@ -356,7 +356,7 @@ rtb_status plan_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
   a.pixels = (long long)p->width * p->height;
   f->metrics = p->collect_metrics ? 1 : 0;
   f->resident = (long long)ctx->sm_count * frame_blocks_per_sm(f->metrics) * 128;
-  // Tail: about two pixels per resident thread are split into single samples.
+  // Tail: about four pixels per resident thread are split into single samples.
   long long tail_pixels = std::min<long long>(a.pixels, (long long)(RTB_TAIL_FACTOR * f->resident));
   set_tail(f, std::min<long long>(tail_pixels, kMaxTailItems / a.spp));
   return RTB_OK;

@@ -61,11 +61,11 @@ def test_render_matches_reference_kernel_without_contraction(wl):
 
 
 @pytest.mark.skipif(not oracle.ref_available("nofmad"), reason="reference kernel not built")
-@pytest.mark.parametrize("size", [(1024, 512, 2), (120, 100, 6000), (96, 64, 1)],
+@pytest.mark.parametrize("size", [(1024, 768, 2), (120, 100, 6000), (96, 64, 1)],
                          ids=["whole-pixel-and-single-sample-lanes", "sample-buffer-cap", "spp1"])
 def test_render_tail_split_matches_reference_kernel(size):
     """The frame's last pixels run one sample per lane and are summed by a second kernel.
-    1024x512 holds more pixels than two per resident thread, so whole-pixel lanes and
+    1024x768 holds more pixels than four per resident thread, so whole-pixel lanes and
     single-sample lanes share the frame; 120x100 at 6000 spp (72M samples) exceeds the
     64M-sample buffer, so only its last 11,184 pixels are split; spp 1 makes every item a
     pixel."""
