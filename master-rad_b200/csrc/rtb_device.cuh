@@ -470,9 +470,13 @@ __device__ __noinline__ void test_all_primitives(const DevScene& S, float3 o, fl
 // the loop condition is a warp vote, so divergent lanes reconverge once per node.  Every lane
 // takes part in the votes, also where lanes hold different scenes and only some of them
 // have a tree (the batch kernel's lanes may belong to different jobs).
-template <bool METRICS>
+//
+// SDEPTH > 0: the first SDEPTH stack entries live in shared memory, in the caller's column
+// `ss` of an [SDEPTH][SSTRIDE] int2 array (node, entry distance bits), so that the entries
+// a traversal uses most stay out of local memory; deeper entries spill to local memory.
+template <bool METRICS, int SDEPTH = 0, int SSTRIDE = 1>
 __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active, Best& b,
-                              TraceCounters* c, int* overflow_flag) {
+                              TraceCounters* c, int* overflow_flag, int2* ss = nullptr) {
   b.t = 1e30f;
   b.order = 0x7FFFFFFF;
   b.type = -1;
@@ -482,8 +486,8 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
   {
     float3 inv = v3(d.x != 0.0f ? 1.0f / d.x : 1e30f, d.y != 0.0f ? 1.0f / d.y : 1e30f,
                     d.z != 0.0f ? 1.0f / d.z : 1e30f);
-    int stack[kStackSize];
-    float estack[kStackSize];
+    int stack[kStackSize - SDEPTH];
+    float estack[kStackSize - SDEPTH];
     int sp = 0;
     int node = (active && bvh) ? 0 : -1;
     bool overflow = false;
@@ -536,8 +540,12 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
           if (next < 0) {
             next = lf;
           } else if (sp < kStackSize) {
-            stack[sp] = lf;
-            estack[sp] = ef;
+            if (SDEPTH > 0 && sp < SDEPTH) {
+              ss[sp * SSTRIDE] = make_int2(lf, __float_as_int(ef));
+            } else {
+              stack[sp - SDEPTH] = lf;
+              estack[sp - SDEPTH] = ef;
+            }
             sp++;
             if (METRICS && (unsigned long long)sp > c->maxstack) c->maxstack = sp;
           } else {
@@ -547,7 +555,17 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
         // Pop the next subtree still closer than the current hit.
         while (next < 0 && sp > 0) {
           --sp;
-          if (estack[sp] <= plim) next = stack[sp];
+          int sn;
+          float se;
+          if (SDEPTH > 0 && sp < SDEPTH) {
+            int2 e = ss[sp * SSTRIDE];
+            sn = e.x;
+            se = __int_as_float(e.y);
+          } else {
+            sn = stack[sp - SDEPTH];
+            se = estack[sp - SDEPTH];
+          }
+          if (se <= plim) next = sn;
         }
         if (--budget < 0) overflow = true;
         node = overflow ? -1 : next;

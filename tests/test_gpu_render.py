@@ -79,6 +79,20 @@ def test_render_tail_split_matches_reference_kernel(size):
     np.testing.assert_array_equal(dev.view(np.int32), ref.view(np.int32))
 
 
+@pytest.mark.skipif(not oracle.ref_available("nofmad"), reason="reference kernel not built")
+def test_render_large_scene_shared_stack_matches_reference_kernel():
+    """A scene whose traversal data exceed 16 MB (400k primitives: about 27 MB of nodes,
+    references and records) renders with the top of each lane's traversal stack in shared
+    memory; the image still equals the reference kernel's bit for bit."""
+    s = synth.hetero_scene(400000, 23, synth.WORKLOAD_IDS["test"], 6)
+    w = synth.Workload("large", s, synth.camera_looking_z((0.0, 0.0, -2.9), 96 / 64), 96, 64, 2,
+                       4, frame_seed=0x5EED, frame_index=1)
+    bvh = oracle.build_bvh(w.scene)
+    dev, _ = _render(w, bvh)
+    ref, _ = oracle.ref_render(w, bvh, variant="nofmad")
+    np.testing.assert_array_equal(dev.view(np.int32), ref.view(np.int32))
+
+
 @pytest.mark.skipif(not oracle.ref_available("fmad"), reason="reference kernel not built")
 def test_render_vs_reference_kernel_as_shipped():
     w = _small_hetero(96, 64, 8, 6)
