@@ -55,9 +55,9 @@ from rtb200.tracer import Context, ResidentScene, build_config, camera_struct, s
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 # dram__bytes_read.sum + dram__bytes_write.sum of k_render per sample, from one ncu capture
-# of the same scene at 1024x512x4 spp (profiles/k_render_hetero10k_1024x512x4spp_full.md);
+# of the same scene at 1024x768x4 spp (profiles/k_render_hetero10k_1024x768x4spp_full.md);
 # workloads without a capture report null traffic.
-TRAFFIC_BYTES_PER_SAMPLE = {"hetero": (20.53e6 + 85.28e6) / 2097152}
+TRAFFIC_BYTES_PER_SAMPLE = {"hetero": (22.41e6 + 115.70e6) / 3145728}
 
 
 def parse_args(argv=None):
@@ -596,7 +596,7 @@ def main():
                          "frac": achieved / peak,
                          "traffic": (TRAFFIC_BYTES_PER_SAMPLE[args.workload] * samples_per_frame
                                      if args.workload in TRAFFIC_BYTES_PER_SAMPLE else None),
-                         "traffic_note": ("ncu capture of a 1024x512x4spp frame of the same "
+                         "traffic_note": ("ncu capture of a 1024x768x4spp frame of the same "
                                           "scene, scaled by samples"
                                           if args.workload in TRAFFIC_BYTES_PER_SAMPLE
                                           else "no capture of this workload"),
