@@ -58,6 +58,24 @@ FALLBACK_HBM_GBS = 6650.0
 # of the same scene at 1024x768x4 spp (profiles/k_render_hetero10k_1024x768x4spp_full.md);
 # workloads without a capture report null traffic.
 TRAFFIC_BYTES_PER_SAMPLE = {"hetero": (22.41e6 + 115.70e6) / 3145728}
+# smsp__inst_executed.sum of k_render per sample from the same capture (9.28 G warp
+# instructions for 3,145,728 samples), for the issue bound: warp instructions per second
+# against one instruction per cycle on each of the 4 schedulers of every SM.
+INST_PER_SAMPLE = {"hetero": 9.28e9 / 3145728}
+
+
+def issue_roofline(workload, samples, launch_ms, sm_count, sm_mhz):
+    """The issue bound of the render launch, or None without a capture of this workload."""
+    if workload not in INST_PER_SAMPLE or not sm_mhz or not sm_count:
+        return None
+    inst = INST_PER_SAMPLE[workload] * samples
+    achieved = inst / (launch_ms / 1e3)
+    peak = sm_count * 4 * sm_mhz * 1e6
+    return {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "warp-inst/s",
+            "frac": achieved / peak, "inst_per_launch": inst,
+            "note": "instructions per sample from the ncu capture of a 1024x768x4spp frame of "
+                    "the same scene, scaled by samples; peak = SMs x 4 schedulers x the SM "
+                    "clock sampled during the timed frames"}
 
 
 def parse_args(argv=None):
@@ -605,6 +623,9 @@ def main():
                          "launch_ms": launch_ms,
                          "note": "working set is L2-resident; the bytes are served mostly from "
                                  "L1/L2, so the kernel is latency/issue-bound, not HBM-bound"},
+            "roofline_issue": issue_roofline(
+                args.workload, samples_per_frame, launch_ms, ctx.device_info().sm_count,
+                clock_info.get("sm_mhz") or clock_info.get("sm_max_mhz")),
             "counters_per_sample": {k: float(v) / samples_per_frame for k, v in zip(
                 ["segments", "aabb_tests", "primitive_tests", "sphere", "box", "plane",
                  "affine_sphere", "affine_box", "overflows", "max_stack", "internal_nodes",
