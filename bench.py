@@ -214,6 +214,36 @@ def max_over_ranks(x, device="cuda"):
     return float(t.item())
 
 
+def scenes_of_rank(count, rank, world):
+    """Scene indices a rank renders in the batched workload: round-robin over the ranks."""
+    return list(range(rank, count, world))
+
+
+def init_ranks(world, local):
+    """Selects this rank's GPU and, with more than one rank, joins the NCCL process group."""
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1 and not dist.is_initialized():
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def finish_ranks(world):
+    """Every rank leaves the process group together."""
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def whole_job_rate(world, steps, samples_per_frame, seconds):
     """Msamples/s of the whole job: every rank's frames over the slowest rank's time."""
     return world * steps * samples_per_frame / seconds / 1e6
@@ -258,24 +288,28 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_batched(args):
+def run_batched(args, rank=0, world=1, local=0):
     """The 64-scene batch (primitive counts log-uniform in [1k, 200k], resolutions from
     {256^2, 512^2, 1024^2}, 16 or 64 spp, depth 6): per-scene frames launched back to back
     versus the batch replayed from its CUDA graph after autotuning (one shared-queue kernel
-    over all jobs, or the jobs' own frames spread over concurrent graph branches)."""
+    over all jobs, or the jobs' own frames spread over concurrent graph branches).  With
+    several ranks the scenes are dealt round-robin, each rank batching its own on its GPU;
+    the rate is all 64 scenes' samples over the slowest rank's time."""
     import torch
     from rtb200.batch import Batch
-    torch.cuda.set_device(0)
-    ctx = Context(0)
+    init_ranks(world, local)
+    ctx = Context(local)
     lib = ctx.lib
-    works = synth.batched_workloads()
+    all_works = synth.batched_workloads()
+    total_samples = sum(w.width * w.height * w.spp for w in all_works)
+    works = [all_works[i] for i in scenes_of_rank(len(all_works), rank, world)]
     t0 = time.perf_counter()
     scenes = [ResidentScene.build(ctx, w.scene) for w in works]
     build_ms = sum(r.stats.build_ms for r in scenes)
     build_wall = time.perf_counter() - t0
     outs = [torch.zeros(w.width * w.height * 3, dtype=torch.float32, device="cuda") for w in works]
     samples = sum(w.width * w.height * w.spp for w in works)
-    stream = torch.cuda.Stream()
+    stream = torch.cuda.Stream(device=local)
     sh = C.c_void_p(stream.cuda_stream)
 
     def sequential():
@@ -295,36 +329,44 @@ def run_batched(args):
         for _ in range(args.warmup):
             fn()
         stream.synchronize()
+        barrier(world)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.steps):
             fn()
         e1.record(stream)
         e1.synchronize()
+        barrier(world)
         return e0.elapsed_time(e1) / args.steps
 
-    seq_ms = timed(sequential)
+    seq_ms = max_over_ranks(timed(sequential))
     ref_imgs = [o.cpu().numpy().copy() for o in outs]
-    bat_ms = timed(lambda: batch.render(stream.cuda_stream))
+    bat_ms = max_over_ranks(timed(lambda: batch.render(stream.cuda_stream)))
     same = all(np.array_equal(o.cpu().numpy().view(np.int32), r.view(np.int32))
                for o, r in zip(outs, ref_imgs))
-    line = {"metric": "Msamples/s", "value": samples / (bat_ms / 1e3) / 1e6, "unit": "Msamples/s",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": bat_ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic",
-            "config": {"workload": "batched-64-scenes", "scenes": len(works), "samples": samples,
-                       "primitives": sum(w.scene.bounded_primitive_count() for w in works)},
-            "sequential": {"value": samples / (seq_ms / 1e3) / 1e6, "ms_per_step": seq_ms},
+    differ = max_over_ranks(0.0 if same else 1.0)
+    # each frame or shared-queue launch is followed by its single-sample tail sum
+    launches = max_over_ranks(args.steps * 2 * (len(works) if tuned["branches"] > 0 else 1))
+    line = {"metric": "Msamples/s", "value": total_samples / (bat_ms / 1e3) / 1e6,
+            "unit": "Msamples/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": bat_ms, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "batched-64-scenes", "scenes": len(all_works),
+                       "samples": total_samples,
+                       "primitives": sum(w.scene.bounded_primitive_count() for w in all_works),
+                       "parallelism": ("scenes round-robin over ranks" if world > 1
+                                       else "single GPU")},
+            "sequential": {"value": total_samples / (seq_ms / 1e3) / 1e6, "ms_per_step": seq_ms},
             "batched_over_sequential": seq_ms / bat_ms, "tuning": tuned,
-            "images_identical": bool(same), "device_build_ms_total": build_ms,
-            "build_wall_s": build_wall,
-            # each frame or shared-queue launch is followed by its single-sample tail sum
-            "gpu_launches": args.steps * 2 * (len(works) if tuned["branches"] > 0 else 1)}
-    print(json.dumps(line), flush=True)
+            "images_identical": differ == 0.0, "device_build_ms_total": build_ms,
+            "build_wall_s": build_wall, "gpu_launches": int(launches) * world}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     batch.close()
     for r in scenes:
         r.close()
     ctx.close()
+    finish_ranks(world)
 
 
 def pick_parameters(g, n_albedo, count, rng):
@@ -345,16 +387,18 @@ def pick_parameters(g, n_albedo, count, rng):
     return np.array(out, dtype=np.int64)
 
 
-def run_adjoint(args):
+def run_adjoint(args, rank=0, world=1, local=0):
     """The differentiable workload: 4096-primitive mixed scene, 512x512, 32 spp, depth 6; L2
     image loss against a target rendered with albedos perturbed by N(0, 0.05) (12-uniform
     approximation, clamped to [0, 1]); forward frame vs path-replay backward time, and the
     relative error against central finite differences (h = 1e-3, common random numbers, FP64
-    loss) on 64 random parameters whose gradient is at least 1 % of the largest."""
+    loss) on 64 random parameters whose gradient is at least 1 % of the largest.  One
+    backward pass does not shard: with several ranks each runs an independent replica on its
+    GPU, and the rate is all replicas' samples over the slowest rank's backward time."""
     import torch
     from rtb200.diff import DifferentiableScene
-    torch.cuda.set_device(0)
-    ctx = Context(0)
+    init_ranks(world, local)
+    ctx = Context(local)
     w = synth.adjoint_workload()
     ds = DifferentiableScene(ctx, w.scene, w.width, w.height, w.spp, w.max_depth, w.camera,
                              w.frame_index, w.frame_seed)
@@ -369,7 +413,7 @@ def run_adjoint(args):
     img = torch.empty(n, dtype=torch.float32, device="cuda")
     ga = torch.empty(ds.count * 3, dtype=torch.float32, device="cuda")
     ge = torch.empty(ds.count * 3, dtype=torch.float32, device="cuda")
-    sobj = torch.cuda.Stream()
+    sobj = torch.cuda.Stream(device=local)
     stream = sobj.cuda_stream
 
     def render(alb, emi):
@@ -384,6 +428,7 @@ def run_adjoint(args):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     fwd, bwd = [], []
     torch.cuda.synchronize()
+    barrier(world)
     for i in range(args.warmup + args.steps):
         e0.record(sobj)
         ds.render_into(img.data_ptr(), stream)
@@ -415,20 +460,24 @@ def run_adjoint(args):
         errs.append(abs(g[idx] - fd) / max(abs(fd), 1e-12))
     errs = np.array(errs)
     samples = w.width * w.height * w.spp
-    f_ms, b_ms = statistics.mean(fwd), statistics.mean(bwd)
-    line = {"metric": "Msamples/s", "value": samples / (b_ms / 1e3) / 1e6, "unit": "Msamples/s",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": b_ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic",
+    f_ms = max_over_ranks(statistics.mean(fwd))
+    b_ms = max_over_ranks(statistics.mean(bwd))
+    line = {"metric": "Msamples/s", "value": world * samples / (b_ms / 1e3) / 1e6,
+            "unit": "Msamples/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": b_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "adjoint-4k 512x512 32spp depth6", "materials": ds.count,
-                       "parameters": 6 * ds.count},
+                       "parameters": 6 * ds.count,
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
             "forward_ms": f_ms, "backward_ms": b_ms, "backward_over_forward": b_ms / f_ms,
             "fd_check": {"parameters": int(len(errs)), "h": h, "max_rel_err": float(errs.max()),
                          "median_rel_err": float(np.median(errs))},
-            "gpu_launches": args.steps}
-    print(json.dumps(line), flush=True)
+            "gpu_launches": world * args.steps}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     ds.close()
     ctx.close()
+    finish_ranks(world)
 
 
 def main():
@@ -440,18 +489,14 @@ def main():
         run_reference(args)
         return
     if args.workload == "batched":
-        run_batched(args)
+        run_batched(args, rank, world, local)
         return
     if args.workload == "adjoint":
-        run_adjoint(args)
+        run_adjoint(args, rank, world, local)
         return
     import torch
     import torch.distributed as dist
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    init_ranks(world, local)
     w, wname = make_workload(args.workload, args)
     ctx = Context(local)
     lib = ctx.lib
@@ -639,9 +684,7 @@ def main():
         print(json.dumps(line), flush=True)
     res.close()
     ctx.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    finish_ranks(world)
 
 
 if __name__ == "__main__":

@@ -1,6 +1,7 @@
-"""The two roofline bounds bench.py reports for the render launch: algorithmic bytes against
-the HBM copy bandwidth, and warp instructions against the SMs' issue rate (one instruction
-per cycle on each of an SM's 4 schedulers)."""
+"""Helpers of bench.py: the two roofline bounds it reports for the render launch
+(algorithmic bytes against the HBM copy bandwidth, and warp instructions against the SMs'
+issue rate, one instruction per cycle on each of an SM's 4 schedulers), and how the batched
+workload's scenes are dealt to ranks."""
 import os
 import sys
 
@@ -34,3 +35,23 @@ def test_algorithmic_bytes_formula():
     c = (10, 0, 0, 3, 2, 6, 1, 1, 0, 0, 5, 0, 0, 0)
     want = 64 * 5 + 16 * 3 + 32 * 2 + 48 * 2 + 4 * 7 + 16 * 6 + 100 * 4
     assert bench.algorithmic_bytes(c, 4) == want
+
+
+@pytest.fixture(scope="module")
+def batched_works():
+    from rtb200 import synth
+    return synth.batched_workloads()
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 4, 8])
+def test_batched_scenes_are_dealt_to_ranks_without_overlap(world, batched_works):
+    """--workload batched under N ranks: every one of the 64 scenes is rendered by exactly one
+    rank, so the job's samples are the sum of the ranks' shares."""
+    works = batched_works
+    shares = [bench.scenes_of_rank(len(works), r, world) for r in range(world)]
+    flat = sorted(i for sh in shares for i in sh)
+    assert flat == list(range(len(works)))
+    total = sum(w.width * w.height * w.spp for w in works)
+    assert sum(works[i].width * works[i].height * works[i].spp
+               for sh in shares for i in sh) == total
+    assert max(len(sh) for sh in shares) - min(len(sh) for sh in shares) <= 1
