@@ -87,6 +87,9 @@ def parse_args(argv=None):
     ap.add_argument("--workload", default="hetero", choices=["hetero", "plain", "scale", "batched", "adjoint"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-ref-kernel", action="store_true")
+    ap.add_argument("--ref-frames", type=int, default=0,
+                    help="timed frames of the reference kernel (0: 3, or 1 for the 1M scene)")
     # size overrides for small profiling captures of the same scene
     ap.add_argument("--width", type=int, default=0)
     ap.add_argument("--height", type=int, default=0)
@@ -175,6 +178,53 @@ def algorithmic_bytes(counters, hits):
     bvh_prims = sph + box + asph + abox
     return (64 * internal + 16 * sph + 32 * box + 48 * (asph + abox) + 4 * bvh_prims
             + 16 * plane + (64 + 36) * hits)
+
+
+def ref_kernel_leg(w, tree, frames, flush_bytes):
+    """The reference's own renderKernel (extracted from GpuKernelSources.java and built for
+    sm_100a by oracle/build_oracle.py) on the same frame, tree, seeds and camera, launched
+    with renderSample's plan (one launch per (sample, tile), 16x16 blocks, tiles of at most
+    262,144 pixels); CUDA events around each frame, the same L2 flush written before each
+    frame outside the events.  Both builds: NVRTC's default (contraction on, the reference
+    as shipped) and without contraction (the build this library's images equal bit for
+    bit).  A checker leg outside the timed region: returns None when the reference kernel
+    was not built."""
+    from oracle import oracle
+    if not oracle.ref_available("fmad"):
+        return None
+    samples = w.width * w.height * w.spp
+    out = {"unit": "Msamples/s", "frames": frames,
+           "launches_per_frame": w.spp * _ref_tiles(w.width, w.height),
+           "launch_plan": "renderSample: one renderKernel launch per (sample, tile), 16x16 "
+                          "blocks, tiles of <= 262144 pixels",
+           "l2": "flushed before each frame outside the events"}
+    for variant in ("fmad", "nofmad"):
+        if not oracle.ref_available(variant):
+            continue
+        _, ms = oracle.ref_render(w, tree, warmup=1, frames=frames, variant=variant,
+                                  flush_bytes=flush_bytes)
+        out[variant] = {"value": samples * frames / (ms / 1e3) / 1e6,
+                        "ms_per_frame": ms / frames}
+    out["value"] = out["fmad"]["value"]
+    out["variant"] = "fmad: NVRTC's default contraction, the reference as shipped"
+    return out
+
+
+def _ref_tiles(width, height, per_launch=262144):
+    """GpuLaunchProvenance.renderTileLayout (GpuLaunchProvenance.java:44-60): tile count."""
+    tw = min(width, per_launch)
+    th = min(height, max(1, per_launch // tw))
+    return (1 + (width - 1) // tw) * (1 + (height - 1) // th)
+
+
+class _Tree:
+    """A downloaded device tree in the reference's flattened layout, shaped for the oracle."""
+
+    def __init__(self, arrays):
+        self.node_bounds, self.node_data, self.refs, self.roots = arrays
+        self.node_count = len(self.node_data) // 4
+        self.ref_count = len(self.refs)
+        self.root_count = len(self.roots)
 
 
 def cpu_baseline(w, rows, threads=0):
@@ -369,30 +419,61 @@ def run_batched(args, rank=0, world=1, local=0):
     finish_ranks(world)
 
 
-def pick_parameters(g, n_albedo, count, rng):
-    """Random parameters for the finite-difference check: half albedo, half emission, from
-    those whose gradient is at least 1e-2 (else 1e-3, 1e-4) of the largest in their group --
-    smaller gradients are below the finite difference's FP32 image noise."""
-    out = []
-    for lo, hi in ((0, n_albedo), (n_albedo, len(g))):
-        grp = np.abs(g[lo:hi])
-        if grp.size == 0 or grp.max() == 0:
-            continue
-        for frac in (1e-2, 1e-3, 1e-4):
-            cand = np.nonzero(grp >= frac * grp.max())[0]
-            if len(cand) >= count // 2:
-                break
-        take = min(count // 2, len(cand))
-        out.extend((lo + rng.choice(cand, size=take, replace=False)).tolist())
-    return np.array(out, dtype=np.int64)
+FD_SMALL = 1e-3  # |FD| below this fraction of its group's largest gradient counts as small
+
+
+def fd_check(g, n_albedo, loss, alb0, emi0, count, rng, h=1e-3):
+    """Central finite differences (step h, common random numbers: every render uses the same
+    frame seed) on ``count`` parameters drawn uniformly without replacement from all albedo
+    and emission components, against the adjoint's gradient ``g`` (albedo components first).
+    ``loss(albedo, emission)`` returns the FP64 image loss.
+
+    Gradients far below their group's largest (|FD| < FD_SMALL x max) are reported apart:
+    for those a relative error is dominated by the FP32 rounding of the image and of the
+    gradient sums, so they are judged by their absolute error against the group's scale.
+
+    Albedo components of materials whose albedo is zero in all three channels (emitters) are
+    not drawn: there the path ends (the lobe weights sum to zero), and any positive albedo
+    continues it, so the image has no derivative at that point."""
+    dead = np.repeat(np.all(alb0.reshape(-1, 3) == 0.0, axis=1), 3)
+    cand = np.concatenate([np.nonzero(~dead)[0], n_albedo + np.arange(len(g) - n_albedo)])
+    idx = rng.choice(cand, size=min(count, len(cand)), replace=False)
+    n_total = len(cand)
+    scale = np.array([np.abs(g[:n_albedo]).max(initial=0.0),
+                      np.abs(g[n_albedo:]).max(initial=0.0)])
+    rows = []
+    for i in idx:
+        alb, emi = alb0.copy(), emi0.copy()
+        arr, k = (alb, i) if i < n_albedo else (emi, i - n_albedo)
+        flat = arr.reshape(-1)
+        v = flat[k]
+        flat[k] = v + h
+        lp = loss(alb, emi)
+        flat[k] = v - h
+        lm = loss(alb, emi)
+        fd = (lp - lm) / (2 * h)
+        grp = 0 if i < n_albedo else 1
+        rows.append((int(i), grp, float(g[i]), fd, float(scale[grp])))
+    large = [r for r in rows if abs(r[3]) >= FD_SMALL * r[4] and r[4] > 0]
+    small = [r for r in rows if not (abs(r[3]) >= FD_SMALL * r[4] and r[4] > 0)]
+    rel = np.array([abs(r[2] - r[3]) / abs(r[3]) for r in large])
+    absn = np.array([abs(r[2] - r[3]) / r[4] if r[4] > 0 else abs(r[2] - r[3]) for r in small])
+    return {"parameters": len(rows), "drawn_from": n_total, "h": h,
+            "large": {"count": len(large),
+                      "max_rel_err": float(rel.max()) if len(rel) else 0.0,
+                      "median_rel_err": float(np.median(rel)) if len(rel) else 0.0},
+            "small": {"count": len(small), "threshold": "|FD| < %g x group max" % FD_SMALL,
+                      "max_abs_err_over_group_max": float(absn.max()) if len(absn) else 0.0,
+                      "exact_zero": int(sum(1 for r in small if r[2] == 0.0 and r[3] == 0.0))},
+            "rows": rows}
 
 
 def run_adjoint(args, rank=0, world=1, local=0):
     """The differentiable workload: 4096-primitive mixed scene, 512x512, 32 spp, depth 6; L2
     image loss against a target rendered with albedos perturbed by N(0, 0.05) (12-uniform
     approximation, clamped to [0, 1]); forward frame vs path-replay backward time, and the
-    relative error against central finite differences (h = 1e-3, common random numbers, FP64
-    loss) on 64 random parameters whose gradient is at least 1 % of the largest.  One
+    error against central finite differences (h = 1e-3, common random numbers, FP64 loss) on
+    64 parameters drawn uniformly from all albedo and emission components (fd_check).  One
     backward pass does not shard: with several ranks each runs an independent replica on its
     GPU, and the rate is all replicas' samples over the slowest rank's backward time."""
     import torch
@@ -444,21 +525,9 @@ def run_adjoint(args, rank=0, world=1, local=0):
             bwd.append(e0.elapsed_time(e1))
     sobj.synchronize()
     g = np.concatenate([ga.cpu().numpy(), ge.cpu().numpy()]).astype(np.float64)
-    pick = pick_parameters(g, ga.numel(), 64, np.random.default_rng(1))
-    h = 1e-3
-    errs = []
-    for idx in pick:
-        alb, emi = alb0.copy(), emi0.copy()
-        arr, k = (alb, idx) if idx < alb.size else (emi, idx - alb.size)
-        flat = arr.reshape(-1)
-        v = flat[k]
-        flat[k] = v + h
-        lp = float(np.sum((render(alb, emi) - target) ** 2))
-        flat[k] = v - h
-        lm = float(np.sum((render(alb, emi) - target) ** 2))
-        fd = (lp - lm) / (2 * h)
-        errs.append(abs(g[idx] - fd) / max(abs(fd), 1e-12))
-    errs = np.array(errs)
+    fd = fd_check(g, ga.numel(), lambda a, e: float(np.sum((render(a, e) - target) ** 2)),
+                  alb0, emi0, 64, np.random.default_rng(1))
+    fd.pop("rows")
     samples = w.width * w.height * w.spp
     f_ms = max_over_ranks(statistics.mean(fwd))
     b_ms = max_over_ranks(statistics.mean(bwd))
@@ -470,8 +539,7 @@ def run_adjoint(args, rank=0, world=1, local=0):
                        "parameters": 6 * ds.count,
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "forward_ms": f_ms, "backward_ms": b_ms, "backward_over_forward": b_ms / f_ms,
-            "fd_check": {"parameters": int(len(errs)), "h": h, "max_rel_err": float(errs.max()),
-                         "median_rel_err": float(np.median(errs))},
+            "fd_check": fd,
             "gpu_launches": world * args.steps}
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -681,6 +749,14 @@ def main():
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        if world == 1 and not args.no_ref_kernel:
+            frames = args.ref_frames or (1 if args.workload == "scale" else 3)
+            rk = ref_kernel_leg(w, _Tree(res.download_bvh()), frames, flush.numel() * 4)
+            if rk is not None:
+                line["ref_kernel"] = rk
+                line["vs_ref_kernel"] = value / rk["value"]
+                line["vs_ref_kernel_nofmad"] = value / rk["nofmad"]["value"] \
+                    if "nofmad" in rk else None
         print(json.dumps(line), flush=True)
     res.close()
     ctx.close()

@@ -256,8 +256,9 @@ RTB_API rtb_status rtb_batch_destroy(rtb_context* ctx, rtb_batch* batch);
  * in a fixed array of RTB_STATIC_REPLAY_MAX_RAYS rays inside the library, and the call makes
  * no cudaMalloc/cudaFree or other allocation.  Every GPU that loads the library holds that
  * array (about 3.4 MB) until exit.  The first call on a device looks up the array's address
- * (so make it before any stream capture).  Calls share the array: calls that overlap on the
- * GPU race.  Returns RTB_ERR_LIMIT for ray_count > RTB_STATIC_REPLAY_MAX_RAYS.  Runs on the
+ * (so make it before any stream capture) and keeps it for the process: after a
+ * cudaDeviceReset of that device the address is stale, so do not call this entry point on a
+ * device the process has reset.  Calls share the array: calls that overlap on the GPU race.  Returns RTB_ERR_LIMIT for ray_count > RTB_STATIC_REPLAY_MAX_RAYS.  Runs on the
  * scene's device on the calling thread's per-thread default stream and returns when the
  * host outputs are written. */
 #define RTB_STATIC_REPLAY_MAX_RAYS 65536
@@ -308,8 +309,12 @@ RTB_API rtb_status rtb_calibrate_costs(rtb_context* ctx, const rtb_calibration_w
                                        const rtb_calibration_params* params,
                                        rtb_calibration_result* result);
 
-/* Host-writable abort: running persistent kernels of this context stop at their next
- * work fetch and the call returns RTB_ERR_WATCHDOG.  Cleared by the next render call. */
+/* Host abort (no reference counterpart; the reference has only its launch watchdog).
+ * Every render, batch and backward launch of this context submitted before this call
+ * (running or still queued) stops at its next work fetch; work submitted after it is not
+ * affected.  A stopped frame leaves the pixels it never fetched unwritten; rtb_render_sample
+ * then returns RTB_ERR_WATCHDOG.  May be called from any thread while another thread holds
+ * the context in a render call. */
 RTB_API rtb_status rtb_request_abort(rtb_context* ctx);
 
 #ifdef __cplusplus

@@ -72,6 +72,19 @@ rtb_status read_counters(rtb_context* ctx, long long* dst) {
 }
 }  // namespace
 
+namespace rtb {
+namespace {
+__global__ void k_arm_abort(int* words, int generation) {
+  words[1] = generation;
+  words[2] = 0;
+}
+}  // namespace
+
+void arm_abort(rtb_context* ctx, cudaStream_t s) {
+  k_arm_abort<<<1, 1, 0, s>>>(ctx->d_abort, ctx->abort_generation.load());
+}
+}  // namespace rtb
+
 extern "C" {
 
 const char* rtb_status_string(rtb_status s) {
@@ -129,8 +142,8 @@ rtb_status rtb_context_create(int device, rtb_context** out) {
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->order_ev, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_work, 32 * sizeof(unsigned long long));
-  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_abort, sizeof(int));
-  if (e == cudaSuccess) e = cudaMemset(ctx->d_abort, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_abort, 4 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_abort, 0, 4 * sizeof(int));
   if (e != cudaSuccess) {
     rtb_context_destroy(ctx);
     return RTB_ERR_CUDA;
@@ -315,7 +328,7 @@ rtb_status rtb_render_device(rtb_context* ctx, rtb_scene* scene, const rtb_camer
   Guard g(ctx);
   cudaStream_t sm = stream ? (cudaStream_t)stream : ctx->stream;
   ctx_acquire(ctx, sm);
-  cudaMemsetAsync(ctx->d_abort, 0, sizeof(int), sm);
+  arm_abort(ctx, sm);
   rtb_status s = render_frame(ctx, scene, camera, params, rgb_device, sm, false);
   ctx_release(ctx, sm);
   return s;
@@ -332,14 +345,14 @@ rtb_status rtb_render_sample(rtb_context* ctx, rtb_scene* scene, const rtb_camer
   if (!d_rgb) return fail(ctx, RTB_ERR_OUT_OF_MEMORY, "output staging");
   cudaStream_t sm = ctx->stream;
   ctx_acquire(ctx, sm);
-  cudaMemsetAsync(ctx->d_abort, 0, sizeof(int), sm);
+  arm_abort(ctx, sm);
   rtb_status s = render_frame(ctx, scene, camera, params, d_rgb, sm, true);
   ctx_release(ctx, sm);
   if (s != RTB_OK) return s;
   cudaError_t e = cudaEventSynchronize(ctx->ev1);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "render");
-  int aborted = 0;
-  cudaMemcpy(&aborted, ctx->d_abort, sizeof(int), cudaMemcpyDeviceToHost);
+  int aborted = 0;  // abort word [2]: the kernel stopped fetching work
+  cudaMemcpy(&aborted, ctx->d_abort + 2, sizeof(int), cudaMemcpyDeviceToHost);
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
   auto tc = Clock::now();
@@ -370,14 +383,21 @@ rtb_status rtb_last_frame_stats(rtb_context* ctx, rtb_frame_stats* out) {
 
 rtb_status rtb_request_abort(rtb_context* ctx) {
   if (!ctx) return RTB_ERR_INVALID_ARGUMENT;
-  // Not under the context mutex: it must reach a render that holds it.
-  int one = 1;
+  // Not under the context mutex: it must reach a render that holds it.  Requests are
+  // serialised among themselves so that generations land in increasing order, and a
+  // generation is published (taken by later submissions) only once it is on the device:
+  // work submitted before this call sees a generation above its own and stops; work
+  // submitted after it never does.
+  std::lock_guard<std::mutex> lock(ctx->abort_mu);
+  int next = ctx->abort_generation.load() + 1;
   cudaSetDevice(ctx->device);
   cudaStream_t s;
   if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return RTB_ERR_CUDA;
-  cudaMemcpyAsync(ctx->d_abort, &one, sizeof(int), cudaMemcpyHostToDevice, s);
-  cudaStreamSynchronize(s);
+  cudaError_t e = cudaMemcpyAsync(ctx->d_abort, &next, sizeof(int), cudaMemcpyHostToDevice, s);
+  cudaError_t e2 = cudaStreamSynchronize(s);
   cudaStreamDestroy(s);
+  if (e != cudaSuccess || e2 != cudaSuccess) return RTB_ERR_CUDA;
+  ctx->abort_generation.store(next);
   return RTB_OK;
 }
 

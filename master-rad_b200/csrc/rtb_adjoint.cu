@@ -35,7 +35,7 @@ struct AdjointArgs {
   float* grad_emission;  // 3 per material
   long long pixels;
   unsigned long long* queue;
-  const int* abort_flag;
+  int* abort_flag;  // the context's abort words (abort_raised)
 };
 
 __device__ __forceinline__ float luminance(float3 c) {  // K:181-183
@@ -113,8 +113,8 @@ __global__ void __launch_bounds__(128, 6) k_adjoint(AdjointArgs a) {
       unsigned long long basep = 0;
       int leader = __ffs(need_mask) - 1;
       if (lane == leader)
-        basep = (*(volatile const int*)a.abort_flag) ? (unsigned long long)a.pixels
-                                                     : atomicAdd(a.queue, (unsigned long long)__popc(need_mask));
+        basep = abort_raised(a.abort_flag) ? (unsigned long long)a.pixels
+                                           : atomicAdd(a.queue, (unsigned long long)__popc(need_mask));
       basep = __shfl_sync(0xFFFFFFFFu, basep, leader);
       if (need) {
         long long p = (long long)basep + __popc(need_mask & ((1u << lane) - 1u));
@@ -320,7 +320,7 @@ rtb_status rtb_render_backward(rtb_context* ctx, rtb_scene* scene, const rtb_cam
   a.abort_flag = ctx->d_abort;
   size_t gbytes = (size_t)scene->dev.material_count * 3 * sizeof(float);
   cudaMemsetAsync(ctx->d_work, 0, sizeof(unsigned long long), sm);
-  cudaMemsetAsync(ctx->d_abort, 0, sizeof(int), sm);
+  arm_abort(ctx, sm);
   cudaMemsetAsync(grad_albedo_device, 0, gbytes, sm);
   cudaMemsetAsync(grad_emission_device, 0, gbytes, sm);
   int bps = 1;

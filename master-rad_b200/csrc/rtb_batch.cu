@@ -91,7 +91,7 @@ template <int THREADS>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_batch(const BatchJob* jobs, int njobs,
                                                                    long long total, float* tail,
                                                                    unsigned long long* queue,
-                                                                   const int* abort_flag) {
+                                                                   int* abort_flag) {
   __shared__ long long s_begin[kMaxSharedJobs];
   const int nshared = njobs < kMaxSharedJobs ? njobs : kMaxSharedJobs;
   for (int j = threadIdx.x; j < nshared; j += THREADS) s_begin[j] = jobs[j].begin;
@@ -113,8 +113,8 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_batch(const BatchJo
       unsigned long long basep = 0;
       int leader = __ffs(need_mask) - 1;
       if (lane == leader)
-        basep = (*(volatile const int*)abort_flag) ? (unsigned long long)total
-                                                   : atomicAdd(queue, (unsigned long long)__popc(need_mask));
+        basep = abort_raised(abort_flag) ? (unsigned long long)total
+                                         : atomicAdd(queue, (unsigned long long)__popc(need_mask));
       basep = __shfl_sync(0xFFFFFFFFu, basep, leader);
       if (need) {
         long long g = (long long)basep + __popc(need_mask & ((1u << lane) - 1u));
@@ -247,12 +247,12 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_batch(const BatchJo
 }
 
 // One thread per tail pixel of the batch: the in-order FP32 sum of its samples, scaled as in
-// k_batch.  An aborted batch leaves its tail pixels unwritten.
+// k_batch.  A batch whose kernel stopped on an abort leaves its tail pixels unwritten.
 __global__ void __launch_bounds__(256) k_sum_batch_tail(const BatchJob* jobs, int njobs,
                                                         const float* __restrict__ tail,
                                                         int tail_pixels, const int* abort_flag) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= tail_pixels || *(volatile const int*)abort_flag) return;
+  if (q >= tail_pixels || abort_stopped(abort_flag)) return;
   int lo = 0, hi = njobs - 1;  // last job with tail_begin <= q
   while (lo < hi) {
     int mid = (lo + hi + 1) >> 1;
@@ -567,7 +567,7 @@ rtb_status rtb_batch_render(rtb_context* ctx, rtb_batch* B, void* stream) {
   cudaSetDevice(ctx->device);
   cudaStream_t sm = stream ? (cudaStream_t)stream : ctx->stream;
   ctx_acquire(ctx, sm);
-  cudaMemsetAsync(ctx->d_abort, 0, sizeof(int), sm);
+  arm_abort(ctx, sm);  // outside the graph: its kernels read the words, never write [1]
   cudaError_t e = cudaGraphLaunch(B->exec, sm);
   ctx_release(ctx, sm);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "batch graph launch");
@@ -598,6 +598,7 @@ rtb_status rtb_batch_autotune(rtb_context* ctx, rtb_batch* B, int repeats, rtb_b
     if (s != RTB_OK) break;
     double total = 0.0;
     for (int r = 0; r <= repeats && s == RTB_OK; ++r) {  // first run warms up
+      arm_abort(ctx, sm);
       cudaEventRecord(ctx->ev0, sm);
       s = enqueue(ctx, B, sm);
       if (s != RTB_OK) break;

@@ -96,6 +96,20 @@ __device__ __forceinline__ float3 normalize_transformed(float3 v) {  // K:101-11
 }
 
 // ---------------------------------------------------------------- RNG (K:165-179)
+// Host abort words, three ints in device memory owned by the context:
+//   [0] the abort generation, raised by rtb_request_abort;
+//   [1] the generation that was current when the running work was submitted, written in
+//       stream order just before it (kernel argument of k_arm_abort, so a later abort
+//       request can never be overwritten by it);
+//   [2] set to 1 by a kernel that stopped fetching work because of an abort.
+// A persistent kernel calls abort_raised() before each work fetch.
+__device__ __forceinline__ bool abort_raised(int* w) {
+  if (*(volatile int*)w == *(volatile int*)(w + 1)) return false;
+  *(volatile int*)(w + 2) = 1;
+  return true;
+}
+__device__ __forceinline__ bool abort_stopped(const int* w) { return *(volatile const int*)(w + 2) != 0; }
+
 __device__ __forceinline__ uint32_t hash_u32(uint32_t x) {
   x ^= x >> 17;
   x *= 0xed5ad4bbU;

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -26,7 +27,12 @@ struct rtb_context {
   rtb_frame_stats last{};
   // Small device scratch: [0] pixel queue head (u64), [1..] status words, counters.
   unsigned long long* d_work = nullptr;
-  int* d_abort = nullptr;  // host-written abort flag (device memory)
+  // Abort words in device memory (see abort_raised): [0] generation, [1] generation at
+  // submit, [2] stopped.  abort_generation is the last generation on the device; abort_mu
+  // serialises rtb_request_abort calls.
+  int* d_abort = nullptr;
+  std::atomic<int> abort_generation{0};
+  std::mutex abort_mu;
   // Replay / output staging reused across calls.
   void* d_stage = nullptr;
   size_t stage_bytes = 0;
@@ -65,6 +71,11 @@ inline void ctx_release(rtb_context* ctx, cudaStream_t s) {
   cudaEventRecord(ctx->order_ev, s);
   ctx->order_pending = true;
 }
+
+// Enqueues, on `s`, the write of the current abort generation as the submitted work's own
+// and the clearing of the stopped word.  Every launch of a persistent kernel is preceded by
+// it (outside any graph capture: the generation is a kernel argument).
+void arm_abort(rtb_context* ctx, cudaStream_t s);
 
 // Status helpers.
 rtb_status fail(rtb_context* ctx, rtb_status s, const std::string& msg);

@@ -31,7 +31,7 @@ struct RenderArgs {
   long long items;                 // split + (pixels - split) * spp queue items
   float* tail;                     // RGB of each tail item, item - split order
   unsigned long long* queue;       // work queue head
-  int* abort_flag;                 // host-set abort
+  int* abort_flag;                 // the context's abort words (abort_raised)
   unsigned long long* counters;    // 14 counters (metrics build) + overflow count
 };
 
@@ -91,8 +91,8 @@ __global__ void __launch_bounds__(128, 8) k_render(RenderArgs a) {
       unsigned long long basep = 0;
       int leader = __ffs(need_mask) - 1;
       if (lane == leader) {
-        basep = (*(volatile int*)a.abort_flag) ? (unsigned long long)a.items
-                                               : atomicAdd(a.queue, (unsigned long long)__popc(need_mask));
+        basep = abort_raised(a.abort_flag) ? (unsigned long long)a.items
+                                           : atomicAdd(a.queue, (unsigned long long)__popc(need_mask));
       }
       basep = __shfl_sync(0xFFFFFFFFu, basep, leader);
       if (need) {
@@ -231,12 +231,13 @@ __global__ void __launch_bounds__(128, 8) k_render(RenderArgs a) {
 }
 
 // One thread per tail pixel: the in-order FP32 sum of its samples, scaled as in k_render.
-// An aborted frame leaves tail pixels unwritten, like the pixels it never fetched.
+// A frame whose render stopped on an abort leaves tail pixels unwritten, like the pixels it
+// never fetched.
 __global__ void __launch_bounds__(256) k_sum_tail(const float* __restrict__ tail, float* out,
                                                  long long split, int tail_pixels, int spp,
                                                  const int* abort_flag) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= tail_pixels || *(volatile const int*)abort_flag) return;
+  if (q >= tail_pixels || abort_stopped(abort_flag)) return;
   const float* s = tail + 3 * (size_t)q * spp;
   float3 acc = v3(s[0], s[1], s[2]);
   for (int i = 1; i < spp; i++) acc = add(acc, v3(s[3 * i], s[3 * i + 1], s[3 * i + 2]));

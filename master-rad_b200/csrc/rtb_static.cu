@@ -12,10 +12,14 @@
 // (RTB_STATIC_REPLAY_MAX_RAYS x 52 bytes) until the process exits.  Host code cannot use the
 // array's name as a device address, so the first call on each device (with that device
 // current) looks the address up with cudaGetSymbolAddress and caches it; that first call
-// should come before any stream capture.  Every call on a device shares the one array and
-// the last call's contents stay in it; the output slots of a call are cleared before its
-// launch.  Calls that overlap on the GPU race on the array: issue them from one thread, or
-// serialise them.
+// should come before any stream capture.  The cached address belongs to the device's
+// primary context: after cudaDeviceReset (or anything else that destroys that context and
+// reloads the module) it no longer names the array, so a process that resets a device must
+// not call this entry point on it again.  Every call on a device shares the one array and
+// the last call's contents stay in it; that is harmless here because the trace kernel
+// writes every output record of every ray of the call (flag, distance, order, material and
+// normal, misses included), so no slot of an earlier call is read back.  Calls that overlap
+// on the GPU race on the array: issue them from one thread, or serialise them.
 #include <cstring>
 #include <mutex>
 
@@ -83,9 +87,6 @@ extern "C" rtb_status rtb_trace_replay_static(const rtb_scene* scene, const floa
     float* d_normal = (float*)(base + kRaysBytes + 4 * kWordBytes);
     cudaStream_t sm = cudaStreamPerThread;
     e = cudaMemcpyAsync(d_rays, rays, n * 24, cudaMemcpyHostToDevice, sm);
-    // The array keeps the previous call's records: clear this call's output slots.
-    if (e == cudaSuccess) e = cudaMemsetAsync(d_flags, 0, 4 * kWordBytes, sm);
-    if (e == cudaSuccess) e = cudaMemsetAsync(d_normal, 0, n * 12, sm);
     if (e == cudaSuccess)
       e = launch_trace(scene->dev, use_bvh, d_rays, ray_count, d_flags, d_t, d_order, d_mat, d_normal, sm);
     if (e == cudaSuccess) e = cudaMemcpyAsync(hit_flags, d_flags, n * 4, cudaMemcpyDeviceToHost, sm);

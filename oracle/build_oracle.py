@@ -17,9 +17,13 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_ROOT = "/root/reference"
-KERNEL_SOURCE = os.path.join(
-    REF_ROOT, "src/xyz/marsavic/gfxlab/gpu/GpuKernelSources.java")
+# The reference checkout: RTB_REFERENCE_ROOT, or --reference-root on the command line.
+REF_ROOT = os.environ.get("RTB_REFERENCE_ROOT", "/root/reference")
+KERNEL_SUBPATH = "src/xyz/marsavic/gfxlab/gpu/GpuKernelSources.java"
+
+
+def kernel_source(ref_root=None):
+    return os.path.join(ref_root or REF_ROOT, KERNEL_SUBPATH)
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -45,9 +49,9 @@ def build_cpu(force=False):
     return out
 
 
-def extract_reference_kernel(dst):
+def extract_reference_kernel(dst, ref_root=None):
     """Copies the PATH_TRACER text block (two blocks joined by .concat) to ``dst``."""
-    text = open(KERNEL_SOURCE, encoding="utf-8").read()
+    text = open(kernel_source(ref_root), encoding="utf-8").read()
     m = re.search(r'PATH_TRACER = """\n(.*?)""".concat\("""\n(.*?)"""\);', text, re.S)
     if not m:
         raise RuntimeError("PATH_TRACER text block not found")
@@ -59,14 +63,15 @@ def extract_reference_kernel(dst):
         f.write(body)
 
 
-def build_reference(force=False):
+def build_reference(force=False, ref_root=None):
     ref_dir = os.path.join(HERE, "_ref")
-    if not os.path.exists(KERNEL_SOURCE):
+    ksrc = kernel_source(ref_root)
+    if not os.path.exists(ksrc):
         return None
     src = os.path.join(ref_dir, "ref_kernel.cu")
     harness = os.path.join(HERE, "ref_harness.cu")
-    if force or _stale(src, [KERNEL_SOURCE]):
-        extract_reference_kernel(src)
+    if force or _stale(src, [ksrc]):
+        extract_reference_kernel(src, ref_root)
     outs = {}
     for name, flags in (("fmad", ["-fmad=true"]), ("nofmad", ["-fmad=false"]),
                         ("metrics", ["-fmad=false", "-DGFXLAB_RENDER_METRICS=1"])):
@@ -79,10 +84,13 @@ def build_reference(force=False):
     return outs
 
 
-def build(force=False):
+def build(force=False, ref_root=None):
     build_cpu(force)
-    build_reference(force)
+    build_reference(force, ref_root)
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv)
+    root = None
+    if "--reference-root" in sys.argv:
+        root = sys.argv[sys.argv.index("--reference-root") + 1]
+    build(force="--force" in sys.argv, ref_root=root)

@@ -41,6 +41,7 @@ def lib():
         _lib.orc_render.restype = None
         _lib.orc_cpu_render.restype = C.c_int
         _lib.orc_adjoint.restype = None
+        _lib.orc_primitive_distance.restype = None
     return _lib
 
 
@@ -211,6 +212,22 @@ def ref_trace(scene, rays, bvh=None, use_bvh=True, variant="fmad"):
     return _hits_dict(out)
 
 
+def primitive_distance(scene, rays, orders):
+    """Distance of each ray to the primitive of the given global order (planes included),
+    computed by that primitive's own test in the restatement's uncontracted FP32 arithmetic
+    with no earlier hit; +inf where it misses."""
+    rays = _f32(rays).reshape(-1, 6)
+    orders = _i32(orders).reshape(-1)
+    assert len(orders) == len(rays)
+    arrs, counts = scene.arrays()
+    arrs = [_f32(a) if len(a) else np.zeros(1, np.float32) for a in arrs]
+    ptrs = (C.POINTER(C.c_float) * 6)(*[_fp(a) for a in arrs])
+    out = np.zeros(len(rays), np.float32)
+    lib().orc_primitive_distance(ptrs, _ip(_i32(counts)), _fp(rays), _ip(orders), len(rays),
+                                 _fp(out))
+    return out
+
+
 def _render_params(w):
     return _i32([w.width, w.height, w.spp, w.max_depth, w.frame_index])
 
@@ -228,18 +245,27 @@ def render(workload, bvh=None, use_bvh=True, pixel_begin=0, pixel_end=None):
     return out.reshape(-1, 3)
 
 
-def ref_render(workload, bvh=None, use_bvh=True, warmup=0, frames=1, variant="fmad"):
+def ref_render(workload, bvh=None, use_bvh=True, warmup=0, frames=1, variant="fmad",
+               flush_bytes=0):
     """The reference's renderKernel with renderSample's launch plan; returns (image (H*W,3),
-    summed CUDA-event milliseconds of the timed frames)."""
+    summed CUDA-event milliseconds of the timed frames).  With ``flush_bytes`` > 0 every
+    timed frame has its own events and a buffer of that size is written before it, outside
+    the events (an L2 flush)."""
     w = workload
     sa = _SceneArgs(w.scene, bvh, use_bvh)
     cam = _f32(w.camera.packed())
     bg = _f32(w.scene.background)
     out = np.zeros(3 * w.width * w.height, np.float32)
     ms = C.c_double(0.0)
-    rc = ref_lib(variant).ref_render(*sa.args(), _fp(cam), _fp(bg), _ip(_render_params(w)),
-                                     C.c_ulonglong(w.frame_seed), warmup, frames, _fp(out),
-                                     C.byref(ms))
+    lib_ = ref_lib(variant)
+    if flush_bytes:
+        lib_.ref_render_flushed.restype = C.c_int
+        rc = lib_.ref_render_flushed(*sa.args(), _fp(cam), _fp(bg), _ip(_render_params(w)),
+                                     C.c_ulonglong(w.frame_seed), warmup, frames,
+                                     C.c_ulonglong(flush_bytes), _fp(out), C.byref(ms))
+    else:
+        rc = lib_.ref_render(*sa.args(), _fp(cam), _fp(bg), _ip(_render_params(w)),
+                             C.c_ulonglong(w.frame_seed), warmup, frames, _fp(out), C.byref(ms))
     if rc != 0:
         raise RuntimeError("reference render failed: %d" % rc)
     return out.reshape(-1, 3), ms.value

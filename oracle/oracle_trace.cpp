@@ -770,6 +770,38 @@ void orc_trace(const float* const* arrays, const int* counts, const int* bvh_int
   }
 }
 
+// Distance from each ray r to the one primitive with global order orders[r] (spheres,
+// boxes, affine spheres, affine boxes, planes -- the kernel's tie-break order, K:1003-1017),
+// in this file's uncontracted FP32 arithmetic, as that primitive's own test computes it
+// with no earlier hit (INFINITY where the test misses).  Used to judge whether a hit that
+// another build picked is a near tie of this arithmetic's winner.
+void orc_primitive_distance(const float* const* arrays, const int* counts, const float* rays,
+                            const int* orders, int n, float* out_t) {
+  const int no_bvh[5] = {0, 0, 0, 0, 32};
+  Scene s = make_scene(arrays, counts, no_bvh, nullptr, nullptr, nullptr, nullptr);
+  const int b1 = s.ns, b2 = b1 + s.nb, b3 = b2 + s.nas, b4 = b3 + s.nab, b5 = b4 + s.np;
+  for (int r = 0; r < n; ++r) {
+    f3 o = mk(rays[6 * r], rays[6 * r + 1], rays[6 * r + 2]);
+    f3 d = mk(rays[6 * r + 3], rays[6 * r + 4], rays[6 * r + 5]);
+    int k = orders[r];
+    Hit h;
+    h.t = INFINITY;
+    h.order = 0x7FFFFFFF;
+    bool ok = false;
+    if (k >= 0 && k < b1)
+      ok = trace_sphere(s.spheres + 5 * k, 1, o, d, k, &h);
+    else if (k >= b1 && k < b2)
+      ok = trace_box(s.boxes + 7 * (k - b1), 1, o, d, k, &h);
+    else if (k >= b2 && k < b3)
+      ok = trace_affine_sphere(s.aspheres + 22 * (k - b2), 1, o, d, k, &h);
+    else if (k >= b3 && k < b4)
+      ok = trace_affine_box(s.aboxes + 22 * (k - b3), 1, o, d, k, &h);
+    else if (k >= b4 && k < b5)
+      ok = trace_plane(s.planes + 26 * (k - b4), 1, o, d, k, &h);
+    out_t[r] = ok ? h.t : INFINITY;
+  }
+}
+
 // Renders pixels [pixel_begin, pixel_end) of a width x height image with the
 // renderKernel sample loop: samples 0..spp-1 in order, FP32 running sum, scaled by
 // 1/spp after the last sample (K:1284-1293).  camera: pos, forward, right, up (12 floats);

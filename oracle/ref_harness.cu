@@ -143,11 +143,14 @@ int ref_trace(const float* const* arrays, const int* counts, const int* bvh_ints
 // timed frames (ms, summed) in *kernel_ms and the last frame's image in rgb (3 floats
 // per pixel, may be null).  camera: pos, forward, right, up; params: width, height,
 // spp, max_depth, frame_index.
+// With flush_bytes > 0 each timed frame has its own event pair, and a buffer of that many
+// bytes is written before it, outside the events (an L2 flush, as the library's bench does).
 static int render_frames(const float* const* arrays, const int* counts, const int* bvh_ints,
                          const float* node_bounds, const int* node_data, const int* refs,
                          const int* roots, const float* camera, const float* background,
                          const int* params, unsigned long long frame_seed, int warmup, int frames,
-                         float* rgb, double* kernel_ms, unsigned long long* stats) {
+                         float* rgb, double* kernel_ms, unsigned long long* stats,
+                         size_t flush_bytes = 0) {
   DevScene s;
   int rc = make_scene(&s, arrays, counts, bvh_ints, node_bounds, node_data, refs, roots);
   int width = params[0], height = params[1], spp = params[2], max_depth = params[3];
@@ -163,8 +166,15 @@ static int render_frames(const float* const* arrays, const int* counts, const in
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   double total = 0.0;
+  void* d_flush = nullptr;
+  if (!rc && flush_bytes > 0 && cudaMalloc(&d_flush, flush_bytes) != cudaSuccess) rc = -1;
   for (int f = 0; !rc && f < warmup + frames; ++f) {
-    if (f == warmup) cudaEventRecord(e0);
+    if (d_flush && f >= warmup) {
+      cudaMemsetAsync(d_flush, f & 0xFF, flush_bytes);
+      cudaEventRecord(e0);
+    } else if (f == warmup) {
+      cudaEventRecord(e0);
+    }
     for (int so = 0; so < spp; ++so) {
       for (int t = 0; t < cols * rows; ++t) {
         int c = t % cols, r = t / cols;
@@ -183,8 +193,15 @@ static int render_frames(const float* const* arrays, const int* counts, const in
       }
     }
     if (cudaGetLastError() != cudaSuccess) rc = -2;
+    if (!rc && d_flush && f >= warmup) {
+      cudaEventRecord(e1);
+      cudaEventSynchronize(e1);
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      total += ms;
+    }
   }
-  if (!rc && frames > 0) {
+  if (!rc && frames > 0 && !d_flush) {
     cudaEventRecord(e1);
     cudaEventSynchronize(e1);
     float ms = 0.0f;
@@ -197,6 +214,7 @@ static int render_frames(const float* const* arrays, const int* counts, const in
   if (kernel_ms) *kernel_ms = total;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  cudaFree(d_flush);
   cudaFree(d_out);
   cudaFree(d_stats);
   free_scene(&s);
@@ -210,6 +228,18 @@ int ref_render(const float* const* arrays, const int* counts, const int* bvh_int
                double* kernel_ms) {
   return render_frames(arrays, counts, bvh_ints, node_bounds, node_data, refs, roots, camera,
                        background, params, frame_seed, warmup, frames, rgb, kernel_ms, nullptr);
+}
+
+// As ref_render, with each timed frame timed on its own and an L2 flush of flush_bytes
+// written before it outside the events; *kernel_ms is the sum over the timed frames.
+int ref_render_flushed(const float* const* arrays, const int* counts, const int* bvh_ints,
+                       const float* node_bounds, const int* node_data, const int* refs,
+                       const int* roots, const float* camera, const float* background,
+                       const int* params, unsigned long long frame_seed, int warmup, int frames,
+                       unsigned long long flush_bytes, float* rgb, double* kernel_ms) {
+  return render_frames(arrays, counts, bvh_ints, node_bounds, node_data, refs, roots, camera,
+                       background, params, frame_seed, warmup, frames, rgb, kernel_ms, nullptr,
+                       (size_t)flush_bytes);
 }
 
 // One frame with the kernel's metrics enabled (a build with GFXLAB_RENDER_METRICS): the 14

@@ -102,9 +102,11 @@ def test_render_vs_reference_kernel_as_shipped():
     rel = np.abs(dev - ref) / np.maximum(np.abs(ref), 1e-3)
     per_pixel = rel.max(axis=1)
     outliers = float((per_pixel > 1e-4).mean())
+    print("\npixels above 1e-4 relative: %.3f %%" % (100 * outliers))
     # Path flips at contraction-sensitive near ties; the bulk of the image is within 1e-4.
+    # (At full benchmark size the share is bounded at 0.1 %: test_gpu_configs.py.)
     assert np.median(per_pixel) <= 1e-4
-    assert outliers < 0.25
+    assert outliers <= 1e-2
     rmse = float(np.sqrt(np.mean((dev - ref) ** 2)))
     assert rmse < 0.05 * float(np.sqrt(np.mean(ref ** 2)))
 

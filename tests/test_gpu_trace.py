@@ -5,7 +5,8 @@ Contract (the reference's correctness gate, gfxlab/benchmark/GpuBvhCorrectnessCh
 reference kernel itself built without contraction, hit flags, distances, primitive orders,
 material indices and normals are bit-identical.  Against the reference kernel as NVRTC
 builds it (contraction on), primitive orders may differ only where the two hits are a
-near tie (|t_a - t_b| < 1e-6 * t relative).
+near tie: the differing primitive's distance, computed in the same uncontracted FP32
+arithmetic as ours, is within 1e-6 relative of our hit's.
 """
 import numpy as np
 import pytest
@@ -111,10 +112,11 @@ def test_trace_vs_reference_kernel_as_shipped(ctx, name):
     ref = oracle.ref_trace(scene, rays, bvh, variant="fmad")
     np.testing.assert_array_equal(dev["hit"], ref["hit"])
     bad = np.nonzero(dev["order"] != ref["order"])[0]
-    for i in bad:
-        # the other implementation's hit must be a near tie of ours
-        alt = oracle.trace(scene, rays[i:i + 1], bvh)
-        assert abs(float(ref["t"][i]) - float(dev["t"][i])) <= 1e-6 * max(1.0, abs(float(dev["t"][i]))) * 4
+    # the other build's winner, measured in the one arithmetic that picked ours (the
+    # uncontracted FP32 restatement), must be a near tie of our hit
+    alt = oracle.primitive_distance(scene, rays[bad], ref["order"][bad]).astype(np.float64)
+    t_dev = dev["t"][bad].astype(np.float64)
+    assert np.all(np.abs(alt - t_dev) < 1e-6 * np.abs(t_dev))
     hit = dev["hit"] == 1
     rel = np.abs(dev["t"][hit] - ref["t"][hit]) / np.maximum(1.0, np.abs(ref["t"][hit]))
     assert rel.max() < 1e-4  # the correctness gate's distance tolerance

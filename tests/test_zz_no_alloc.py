@@ -59,6 +59,41 @@ def test_static_replay_matches_allocating_replay_twice():
         ctx.close()
 
 
+def _free_device_bytes():
+    """cudaMemGetInfo's free bytes for the current device, through the CUDA runtime."""
+    torch = pytest.importorskip("torch")
+    free, _ = torch.cuda.mem_get_info(0)
+    return free
+
+
+def test_static_replay_full_array_and_no_allocation():
+    """A call with exactly RTB_STATIC_REPLAY_MAX_RAYS rays fills the last slot of every
+    section and still equals rtb_trace_replay bit for bit.  Once the array is set up (first
+    call on the device), further calls leave the device's free memory unchanged: the call
+    allocates nothing."""
+    ctx = Context(0)
+    try:
+        scene = synth.hetero_scene(3000, 31, synth.WORKLOAD_IDS["test"], 12)
+        rs = ResidentScene.build(ctx, scene)
+        n = N.STATIC_REPLAY_MAX_RAYS
+        cam = synth.camera_looking_z((0.0, 0.0, -2.9))
+        rays = np.concatenate([synth.primary_grid(cam, 256, 128),
+                               synth.random_rays(n - 256 * 128, 47)])
+        assert len(rays) == n
+        _same(_replay(ctx, rs, rays, True), _replay(ctx, rs, rays, False))
+        _replay(ctx, rs, rays[:100], True)  # warm: array set up, kernels loaded
+        before = _free_device_bytes()
+        outs = [_replay(ctx, rs, rays[:k], True) for k in (n, 1, 777, n)]
+        after = _free_device_bytes()
+        assert after == before, (before, after)
+        want = _replay(ctx, rs, rays, False)
+        _same(outs[-1], want)
+        _same(outs[2], {k: v[:777 * (3 if k == "normal" else 1)] for k, v in want.items()})
+        rs.close()
+    finally:
+        ctx.close()
+
+
 def test_static_replay_rejects_more_rays_than_its_array():
     ctx = Context(0)
     try:
