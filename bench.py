@@ -88,6 +88,10 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ref-kernel", action="store_true")
+    ap.add_argument("--split", default="rows", choices=["rows", "frames"],
+                    help="with N > 1 GPUs: rows -- every step is one frame whose rows are dealt "
+                         "out across the ranks and all-gathered (strong scaling); frames -- "
+                         "every rank renders its own frames (weak scaling)")
     ap.add_argument("--ref-frames", type=int, default=0,
                     help="timed frames of the reference kernel (0: 3, or 1 for the 1M scene)")
     # size overrides for small profiling captures of the same scene
@@ -617,13 +621,38 @@ def main():
     # every segment ends in at most one material fetch: an upper bound for the hit bytes
     bytes_per_frame = algorithmic_bytes([int(v) for v in cnt], int(cnt[0]))
 
+    # ---- a step: this rank's own frame, or (rows split) this rank's rows of one frame
+    #      shared by all ranks followed by the all-gather of every rank's rows
+    split_rows = world > 1 and args.split == "rows"
+    if split_rows:
+        from rtb200 import split
+        k_rows = split.band_rows(w.height, world)
+        band = torch.zeros(k_rows * w.width * 3, dtype=torch.float32, device="cuda")
+        gathered = torch.empty(world * band.numel(), dtype=torch.float32, device="cuda")
+
+        def step(frame):
+            p = params(frame)
+            ctx.check(lib.rtb_render_rows_device(ctx.handle, res.handle, C.byref(cam),
+                                                 C.byref(p), rank, world,
+                                                 C.c_void_p(band.data_ptr()), sh))
+            dist.all_gather_into_tensor(gathered, band)
+            out.copy_(split.assemble(gathered, w.height, w.width, world).reshape(-1))
+
+        def step_frame(i, offset=0):  # every rank renders the same frame
+            return frame_index(0, i, offset)
+    else:
+        step = render
+
+        def step_frame(i, offset=0):
+            return frame_index(rank, i, offset)
+
     # ---- warm-up
     for i in range(args.warmup):
         with torch.cuda.stream(stream):
-            render(frame_index(rank, i, 1000))
+            step(step_frame(i, 1000))
     stream.synchronize()
 
-    # ---- timed region: K frames, events around each render launch, L2 flushed between
+    # ---- timed region: K steps, events around each step on its stream, L2 flushed between
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     clocks = ClockSampler(local)
@@ -635,7 +664,7 @@ def main():
         with torch.cuda.stream(stream):
             flush.zero_()
             starts[i].record(stream)
-            render(frame_index(rank, i))
+            step(step_frame(i))
             ends[i].record(stream)
     torch.cuda.synchronize()
     if world > 1:
@@ -645,9 +674,11 @@ def main():
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = float(sum(step_ms))
     total_ms = max_over_ranks(total_ms)
-    value = whole_job_rate(world, args.steps, samples_per_frame, total_ms / 1e3)
+    frames_per_step = 1 if split_rows else world
+    value = whole_job_rate(frames_per_step, args.steps, samples_per_frame, total_ms / 1e3)
     launch_ms = statistics.mean(step_ms)
-    achieved = bytes_per_frame / (launch_ms / 1e3) / 1e9
+    # the roofline is one GPU's kernel: with the rows split each rank runs 1/N of the frame
+    achieved = (bytes_per_frame / world if split_rows else bytes_per_frame) / (launch_ms / 1e3) / 1e9
     peak, peak_kind = peak_hbm()
 
     # ---- e2e through the C ABI with pinned host buffers: upload + device build + render +
@@ -666,19 +697,34 @@ def main():
     bc = build_config(w.scene.config)
     e2e_times = []
     for i in range(0 if args.no_e2e else args.warmup + args.steps):
+        if split_rows:
+            dist.barrier()
         t0 = time.perf_counter()
         h = C.c_void_p()
         st = N.BvhStats()
         ctx.check(lib.rtb_scene_build(ctx.handle, C.byref(d), C.byref(bc), C.byref(h), C.byref(st)))
-        p = params(frame_index(rank, i, 500))
-        ctx.check(lib.rtb_render_sample(ctx.handle, h, C.byref(cam), C.byref(p),
-                                        C.cast(C.c_void_p(img.data_ptr()), N.FP)))
+        if split_rows:
+            # this rank's rows, the all-gather, and the whole frame read back on rank 0
+            p = params(frame_index(0, i, 500))
+            with torch.cuda.stream(stream):
+                ctx.check(lib.rtb_render_rows_device(ctx.handle, h, C.byref(cam), C.byref(p),
+                                                     rank, world, C.c_void_p(band.data_ptr()),
+                                                     sh))
+                dist.all_gather_into_tensor(gathered, band)
+                if rank == 0:
+                    img.copy_(split.assemble(gathered, w.height, w.width, world).reshape(-1),
+                              non_blocking=True)
+            stream.synchronize()
+        else:
+            p = params(frame_index(rank, i, 500))
+            ctx.check(lib.rtb_render_sample(ctx.handle, h, C.byref(cam), C.byref(p),
+                                            C.cast(C.c_void_p(img.data_ptr()), N.FP)))
         lib.rtb_scene_destroy(ctx.handle, h)
         if i >= args.warmup:
             e2e_times.append(time.perf_counter() - t0)
     e2e_total = sum(e2e_times) if e2e_times else float("nan")
     e2e_total = max_over_ranks(e2e_total)
-    e2e_value = whole_job_rate(world, args.steps, samples_per_frame, e2e_total)
+    e2e_value = whole_job_rate(frames_per_step, args.steps, samples_per_frame, e2e_total)
 
     line = None
     if rank == 0:
@@ -705,22 +751,25 @@ def main():
         line = {
             "metric": "Msamples/s", "value": value, "unit": "Msamples/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": "strong" if split_rows else "weak",
+            "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": wname, "primitives": w.scene.bounded_primitive_count(),
                        "planes": w.scene.plane_count, "width": w.width, "height": w.height,
                        "spp": w.spp, "max_depth": w.max_depth, "bvh": "weighted SAH leaf<=4 "
                        "(sphere 1.0, box 1.3, affine 2.1), device-built",
                        "l2": "flushed between frames (256 MiB write outside the events)",
-                       "parallelism": "frames per rank" if world > 1 else "single GPU"},
+                       "parallelism": ("one frame per step, rows r, r+N, ... on rank r, "
+                                       "NCCL all-gather of the rows" if split_rows else
+                                       "frames per rank" if world > 1 else "single GPU")},
             "build_ms": build_ms,
             "build": {"full_sweep_ms": build_ms,
                       "full_sweep_note": "tree identical to the reference Java builder's",
                       "binned_ms": statistics.median(binned_ms), "bins": bins,
                       "binned_note": "binned object SAH, identical to its CPU restatement",
                       "binned_over_full_sah": binned_sah / res.stats.generalized_sah_cost},
-            "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": pixels * 12,
+            "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": h2d * world,
+                    "d2h_bytes_per_step": pixels * 12 * (1 if split_rows else world),
                     "includes": "scene upload from pinned memory + device BVH build + render "
                                 "+ image read-back, per step"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -744,7 +793,7 @@ def main():
                  "affine_sphere", "affine_box", "overflows", "max_stack", "internal_nodes",
                  "leaves", "homogeneous_leaves", "mixed_leaves"], cnt)},
             "clocks": clock_info,
-            "gpu_launches": args.steps * fs.physical_launches,
+            "gpu_launches": args.steps * fs.physical_launches * world,
             "device": ctx.device_info().name,
         }
         if cpu is not None:

@@ -197,6 +197,17 @@ RTB_API rtb_status rtb_render_sample(rtb_context* ctx, rtb_scene* scene, const r
 RTB_API rtb_status rtb_render_device(rtb_context* ctx, rtb_scene* scene, const rtb_camera* camera,
                              const rtb_render_params* params, float* rgb_device, void* stream);
 
+/* One frame's rows first_row, first_row + row_stride, ... (< height), packed densely into
+ * rgb_device (3 floats per pixel, row k of the output = frame row first_row + k*row_stride).
+ * Every pixel equals the same pixel of rtb_render_device's full frame bit for bit (its random
+ * streams are keyed by the frame pixel).  This is the unit of a frame split across GPUs:
+ * rank r of N renders first_row = r, row_stride = N and the rows are gathered (interleaved
+ * rows balance the uneven cost of image regions).  No counterpart in the reference, which
+ * renders a frame on one device (GpuRayTracer.java:796). */
+RTB_API rtb_status rtb_render_rows_device(rtb_context* ctx, rtb_scene* scene, const rtb_camera* camera,
+                                          const rtb_render_params* params, int first_row,
+                                          int row_stride, float* rgb_device, void* stream);
+
 /* GpuRayTracer.lastFrameStats / lastPhysicalKernelLaunchCount (GpuRayTracer.java:294-306). */
 RTB_API rtb_status rtb_last_frame_stats(rtb_context* ctx, rtb_frame_stats* out);
 

@@ -334,6 +334,20 @@ rtb_status rtb_render_device(rtb_context* ctx, rtb_scene* scene, const rtb_camer
   return s;
 }
 
+rtb_status rtb_render_rows_device(rtb_context* ctx, rtb_scene* scene, const rtb_camera* camera,
+                                  const rtb_render_params* params, int first_row, int row_stride,
+                                  float* rgb_device, void* stream) {
+  if (!ctx) return RTB_ERR_INVALID_ARGUMENT;
+  Guard g(ctx);
+  cudaStream_t sm = stream ? (cudaStream_t)stream : ctx->stream;
+  ctx_acquire(ctx, sm);
+  arm_abort(ctx, sm);
+  rtb_status s = render_frame(ctx, scene, camera, params, rgb_device, sm, false, first_row,
+                              row_stride);
+  ctx_release(ctx, sm);
+  return s;
+}
+
 rtb_status rtb_render_sample(rtb_context* ctx, rtb_scene* scene, const rtb_camera* camera,
                              const rtb_render_params* params, float* rgb) {
   if (!ctx) return RTB_ERR_INVALID_ARGUMENT;

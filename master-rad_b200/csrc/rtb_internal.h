@@ -93,9 +93,11 @@ rtb_status scene_create(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_
 void scene_free(rtb_scene* s, cudaStream_t stream);
 
 // rtb_render.cu
+// Rows row0, row0 + row_stride, ... of the frame, packed densely into d_rgb (0, 1: the
+// whole frame).
 rtb_status render_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
                         const rtb_render_params* p, float* d_rgb, cudaStream_t stream,
-                        bool timed);
+                        bool timed, int row0 = 0, int row_stride = 1);
 // One frame's launch, planned apart from where it runs (the batch's frames mode launches
 // many into one graph).  plan_frame validates and sizes; bind_frame gives it a queue head
 // (zeroed before launch), a sample buffer of frame_tail_bytes (nullptr: no single-sample
@@ -105,7 +107,8 @@ struct FramePlan;
 FramePlan* new_frame_plan();
 void delete_frame_plan(FramePlan* f);
 rtb_status plan_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
-                      const rtb_render_params* p, float* d_rgb, FramePlan* f);
+                      const rtb_render_params* p, float* d_rgb, FramePlan* f, int row0 = 0,
+                      int row_stride = 1);
 size_t frame_tail_bytes(const FramePlan* f);
 void bind_frame(FramePlan* f, unsigned long long* queue, float* tail, int* abort_flag,
                 unsigned long long* counters);

@@ -26,7 +26,8 @@ struct RenderArgs {
   int width, height, spp, max_depth, frame_index;
   unsigned long long frame_seed;
   float* out;
-  long long pixels;
+  long long pixels;                // pixels of the output (the frame, or a set of its rows)
+  int row0, row_stride;            // output row k is frame row row0 + k * row_stride
   long long split;                 // pixels [split, pixels) are queued one sample per item
   long long items;                 // split + (pixels - split) * spp queue items
   float* tail;                     // RGB of each tail item, item - split order
@@ -110,7 +111,7 @@ __global__ void __launch_bounds__(128, 8) k_render(RenderArgs a) {
           }
           pixel = p;
           x = (int)(p % a.width);
-          y = (int)(p / a.width);
+          y = a.row0 + (int)(p / a.width) * a.row_stride;
           base_seed = pixel_base_seed(a.frame_seed, a.frame_index,
                                       (uint32_t)y * (uint32_t)a.width + (uint32_t)x);
         }
@@ -355,7 +356,8 @@ void set_tail(FramePlan* f, long long tail_pixels) {
 }  // namespace
 
 rtb_status plan_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
-                      const rtb_render_params* p, float* d_rgb, FramePlan* f) {
+                      const rtb_render_params* p, float* d_rgb, FramePlan* f, int row0,
+                      int row_stride) {
   if (!scene || !cam || !p || !d_rgb) return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "null argument");
   if (p->width < 1 || p->height < 1 || p->samples_per_frame < 1)
     return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "image size and samples must be positive");
@@ -376,8 +378,12 @@ rtb_status plan_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
   a.max_depth = p->max_depth;
   a.frame_index = p->frame_index;
   a.frame_seed = p->frame_seed;
+  if (row0 < 0 || row0 >= p->height || row_stride < 1)
+    return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "first row must be in [0, height) and the stride positive");
   a.out = d_rgb;
-  a.pixels = (long long)p->width * p->height;
+  a.row0 = row0;
+  a.row_stride = row_stride;
+  a.pixels = (long long)p->width * ((p->height - row0 + row_stride - 1) / row_stride);
   f->metrics = p->collect_metrics ? 1 : 0;
   f->shared_stack = traversal_bytes(a.S) > kSharedStackSceneBytes ? kSharedStackDepth : 0;
   f->resident = (long long)ctx->sm_count * frame_blocks_per_sm(f->metrics, f->shared_stack) * 128;
@@ -423,9 +429,10 @@ FramePlan* new_frame_plan() { return new FramePlan(); }
 void delete_frame_plan(FramePlan* f) { delete f; }
 
 rtb_status render_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
-                        const rtb_render_params* p, float* d_rgb, cudaStream_t stream, bool timed) {
+                        const rtb_render_params* p, float* d_rgb, cudaStream_t stream, bool timed,
+                        int row0, int row_stride) {
   FramePlan f;
-  rtb_status s = plan_frame(ctx, scene, cam, p, d_rgb, &f);
+  rtb_status s = plan_frame(ctx, scene, cam, p, d_rgb, &f, row0, row_stride);
   if (s != RTB_OK) return s;
   size_t tail_bytes = frame_tail_bytes(&f);
   if (tail_bytes > ctx->tail_bytes) {

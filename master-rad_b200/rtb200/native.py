@@ -140,6 +140,9 @@ SIGNATURES = {
                                     C.POINTER(RenderParams), FP]),
     "rtb_render_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Camera),
                                     C.POINTER(RenderParams), C.c_void_p, C.c_void_p]),
+    "rtb_render_rows_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Camera),
+                                         C.POINTER(RenderParams), C.c_int, C.c_int, C.c_void_p,
+                                         C.c_void_p]),
     "rtb_last_frame_stats": (C.c_int, [C.c_void_p, C.POINTER(FrameStats)]),
     "rtb_request_abort": (C.c_int, [C.c_void_p]),
     "rtb_calibrate_costs": (C.c_int, [C.c_void_p, C.POINTER(CalibrationWorkload),
