@@ -121,7 +121,10 @@ typedef struct {
   unsigned long long frame_seed;
   int use_bvh;             /* 0: test every primitive (the reference's GPU_LINEAR) */
   int collect_metrics;     /* count traversal work into rtb_frame_stats.counters */
-  int block_size;          /* 0: tuned default */
+  int shared_stack_entries; /* traversal-stack entries per lane kept in shared memory (the
+                              * rest in local memory): 0 picks by scene size (16 for scenes
+                              * over 16 MB of nodes, references and records, else none),
+                              * -1 none, 8 or 16; a tuning knob of the batch autotuner */
 } rtb_render_params;
 
 /* GpuRayTracer.FrameStats (GpuRayTracer.java:79-99).  counters follow the reference's

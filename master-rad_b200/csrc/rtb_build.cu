@@ -11,9 +11,15 @@
 //    stable-partitions each axis array inside the node's range.
 //  * Prefix and suffix bounds are exact min/max unions: segmented scans.
 //  * Prefix and suffix weights are SEQUENTIAL double sums in the reference; with
-//    non-dyadic weights (1.3, 2.1) their rounding depends on the order, so they are summed
-//    sequentially per (node, axis, direction).  With unit weights the sums are exact
-//    integers and are written directly.
+//    non-dyadic weights (1.3, 2.1) their rounding depends on the order.  With unit weights
+//    the sums are exact integers and are written directly.  Otherwise a node of more than
+//    kSeqNodeSize primitives takes its weights from per-type counts (a segmented integer
+//    scan), summed exactly and rounded once, and its costs carry a rigorous bound on how far
+//    the reference's sequentially rounded costs can be from them; its argmin is the
+//    reference's whenever every other candidate's cost minus its bound exceeds the winner's
+//    cost plus its bound.  Smaller nodes, and the few large ones whose winner is not that
+//    clear, sum their weights sequentially per (node, axis, direction), the reference's own
+//    additions in its own order.
 //  * Costs are evaluated in double with the reference's expression order
 //    (nodeArea*cT + A_L*W_L) + A_R*W_R; the argmin keeps the first minimum in
 //    (axis, position) order, as the strict '<' does.
@@ -84,11 +90,15 @@ struct WeightChains {
   double* sw[3];
 };
 
-__global__ void __launch_bounds__(128) k_weights_seq(const WeightChains C, const Nodes N, const int* active,
-                                                     int k) {
+// `nodes` lists the nodes to sum; their number is *count when count is given (a list built
+// on the device; k is then only the grid's bound), else k.
+__global__ void __launch_bounds__(128) k_weights_seq(const WeightChains C, const Nodes N, const int* nodes,
+                                                     int k, const int* count) {
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
+  if (count) k = min(k, *count);
   if (warp >= 6 * k) return;
+  const int* active = nodes;
   int node = active[warp / 6];
   int axis = (warp >> 1) % 3;
   bool suffix = warp & 1;
@@ -127,12 +137,82 @@ __global__ void __launch_bounds__(128) k_weights_seq(const WeightChains C, const
   }
 }
 
+// ---- certified weights for large nodes
+//
+// Nodes above kSeqNodeSize primitives: prefix weight of positions [s, j] = sum over the four
+// primitive types of (count of that type in [s, j]) x (its construction weight), from a
+// segmented inclusive scan of per-type counts, summed in double-double (each product split
+// exactly with fma) and rounded once.  The reference's sequential sum of the same k weights
+// (all positive) is within (k - 1) u of the exact sum relatively (u = 2^-53, the standard
+// bound for recursive summation), so each cost gets a bound on its distance from the
+// reference's: the weight errors times the areas, plus the cost expression's own roundings
+// in both evaluations, doubled for margin.
+constexpr int kSeqNodeSize = 256;
+
+struct TypeCounts {
+  unsigned long long a, b;  // (sphere | box << 32), (affine sphere | affine box << 32)
+};
+struct CountsAdd {
+  __device__ __forceinline__ TypeCounts operator()(const TypeCounts& x, const TypeCounts& y) const {
+    return TypeCounts{x.a + y.a, x.b + y.b};
+  }
+};
+
+__global__ void k_type_onehot(const Prims P, const int* idx, int n, TypeCounts* out) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  int t = P.type[idx[j]];
+  unsigned long long one = 1ULL << (32 * (t & 1));
+  out[j] = t < 2 ? TypeCounts{one, 0ULL} : TypeCounts{0ULL, one};
+}
+
+__device__ __forceinline__ TypeCounts counts_sub(TypeCounts x, TypeCounts y) {
+  return TypeCounts{x.a - y.a, x.b - y.b};
+}
+
+// sum_t c_t w_t, exact in double-double, rounded once: within one rounding of the true sum.
+__device__ __forceinline__ double counts_weight(TypeCounts c, const double* wt) {
+  double cnt[4] = {(double)(c.a & 0xFFFFFFFFULL), (double)(c.a >> 32), (double)(c.b & 0xFFFFFFFFULL),
+                   (double)(c.b >> 32)};
+  double hi = 0.0, lo = 0.0;
+  for (int t = 0; t < 4; ++t) {
+    double p = cnt[t] * wt[t];
+    double pe = fma(cnt[t], wt[t], -p);  // exact: cnt < 2^32 is an integer
+    double s = hi + p;                    // two-sum of hi and p
+    double bp = s - hi;
+    double se = (hi - (s - bp)) + (p - bp);
+    hi = s;
+    lo = lo + (se + pe);
+  }
+  return hi + lo;
+}
+
+struct TypeWeights {
+  double w[4];
+};
+
+__global__ void k_weights_counts(const Nodes N, const int* key, const int* level_of, int level, int n,
+                                 const TypeCounts* scan, TypeWeights W, double* pw, double* sw) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  int node = key[j];
+  if (level_of[node] != level) return;
+  int s = N.start[node], e = N.end[node];
+  if (e - s <= kSeqNodeSize) return;
+  TypeCounts total = scan[e - 1];
+  TypeCounts upto = scan[j];
+  pw[j] = counts_weight(upto, W.w);
+  TypeCounts before = j > s ? scan[j - 1] : TypeCounts{0ULL, 0ULL};
+  sw[j] = counts_weight(counts_sub(total, before), W.w);
+}
+
 // Split cost of every position (GpuScene.java:1482-1485).  cost[j] is the cost of putting
-// positions [s, j) left; +inf marks positions that are not candidates.
+// positions [s, j) left; +inf marks positions that are not candidates.  For nodes whose
+// weights came from counts, bound[j] limits |cost[j] - the reference's cost|.
 __global__ void k_costs(const Prims P, const int* idx, const Nodes N, const int* key,
                         const int* level_of, int level, int axis, int n, const Box* pre,
                         const Box* suf_rev, const double* pw, const double* sw, double traversal,
-                        double* cost) {
+                        int certified, double* cost, double* bound) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   int node = key[j];
@@ -143,12 +223,69 @@ __global__ void k_costs(const Prims P, const int* idx, const Nodes N, const int*
     if (ext > 1.0e-12) {
       Box node_box = pre[e - 1];
       double a = surface_area(node_box) * traversal;
-      double b = surface_area(pre[j - 1]) * pw[j - 1];
-      double d = surface_area(suf_rev[n - 1 - j]) * sw[j];
+      double al = surface_area(pre[j - 1]);
+      double ar = surface_area(suf_rev[n - 1 - j]);
+      double b = al * pw[j - 1];
+      double d = ar * sw[j];
       c = (a + b) + d;
+      if (certified && e - s > kSeqNodeSize) {
+        const double u = 0x1p-53;
+        double kl = (double)(j - s), kr = (double)(e - j);
+        bound[j] = 2.0 * (al * pw[j - 1] * (kl * u) + ar * sw[j] * (kr * u) + 8.0 * u * c);
+      }
     }
   }
   cost[j] = c;
+}
+
+// Nodes of this level split into those summed sequentially (small) and those certified.
+__global__ void k_split_lists(const Nodes N, const int* active, int k, int* small, int* small_count,
+                              int* g_of_node) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= k) return;
+  int node = active[g];
+  g_of_node[node] = g;
+  if (N.end[node] - N.start[node] <= kSeqNodeSize) small[atomicAdd(small_count, 1)] = node;
+}
+
+// The winner's bound, and a cleared failure flag, per certified node.
+__global__ void k_best_bound(const Nodes N, const int* active, int k, const double* best_cost,
+                             const long long* best_flat, const double* bnd0, const double* bnd1,
+                             const double* bnd2, double* best_bound, int* failed) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= k) return;
+  failed[g] = 0;
+  int node = active[g];
+  int s = N.start[node], len = N.end[node] - s;
+  if (len <= kSeqNodeSize || best_cost[g] == CUDART_INF) return;
+  long long flat = best_flat[g];
+  int axis = (int)(flat / len), pos = (int)(flat % len);
+  const double* b = axis == 0 ? bnd0 : axis == 1 ? bnd1 : bnd2;
+  best_bound[g] = b[s + pos];
+}
+
+// A certified node fails when some other candidate could, in the reference's rounding, cost
+// as little as the winner.
+__global__ void k_certify(const Nodes N, const int* key, const int* level_of, int level, int axis,
+                          int n, const int* g_of_node, const double* cost, const double* bound,
+                          const double* best_cost, const long long* best_flat,
+                          const double* best_bound, int* failed) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  int node = key[j];
+  if (level_of[node] != level) return;
+  int s = N.start[node], len = N.end[node] - s;
+  if (len <= kSeqNodeSize) return;
+  double c = cost[j];
+  if (c == CUDART_INF) return;
+  int g = g_of_node[node];
+  if ((long long)axis * len + (j - s) == best_flat[g]) return;
+  if (c - bound[j] <= best_cost[g] + best_bound[g]) failed[g] = 1;
+}
+
+__global__ void k_failed_list(const int* active, int k, const int* failed, int* out, int* count) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < k && failed[g]) out[atomicAdd(count, 1)] = active[g];
 }
 
 struct Cand {
@@ -247,7 +384,7 @@ __global__ void k_argmin_flat(int blocks_total, const double* part_cost, const l
 __global__ void k_decide(const Prims P, IdxSet I, Nodes N, const int* active, int k,
                          const double* best_cost, const long long* best_flat, const Box* pre0,
                          int leaf_size, int* node_counter, int* next_active, int* next_count,
-                         int* level_of, int level, int* stats) {
+                         int* level_of, int level, int* stats, int* largest_child) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= k) return;
   int node = active[g];
@@ -293,6 +430,7 @@ __global__ void k_decide(const Prims P, IdxSet I, Nodes N, const int* active, in
   int q = atomicAdd(next_count, 2);
   next_active[q] = l;
   next_active[q + 1] = r;
+  atomicMax(largest_child, max(pos, n - pos));
 }
 
 __global__ void k_sides(IdxSet I, const Nodes N, const int* key, const int* level_of, int level, int n,
@@ -494,9 +632,13 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
   int* key = W.alloc<int>(n);
   int* key_rev = W.alloc<int>(n);
   Box* boxes = W.alloc<Box>(n);
-  Box* pre = W.alloc<Box>(n);
-  Box* pre0 = W.alloc<Box>(n);
-  Box* suf = W.alloc<Box>(n);
+  Box* pre_ax[3];
+  Box* suf_ax[3];
+  for (int a = 0; a < 3; ++a) {
+    pre_ax[a] = W.alloc<Box>(n);
+    suf_ax[a] = W.alloc<Box>(n);
+  }
+  Box* pre0 = pre_ax[0];
   WeightChains chains;
   for (int a = 0; a < 3; ++a) {
     chains.w[a] = W.alloc<double>(n);
@@ -505,7 +647,19 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
     if (!c.weighted && a > 0) chains.pw[a] = chains.pw[0];
   }
   double* cost[3];
-  for (int a = 0; a < 3; ++a) cost[a] = W.alloc<double>(n);
+  double* bound[3];
+  for (int a = 0; a < 3; ++a) {
+    cost[a] = W.alloc<double>(n);
+    bound[a] = c.weighted ? W.alloc<double>(n) : nullptr;
+  }
+  TypeCounts* onehot = c.weighted ? W.alloc<TypeCounts>(n) : nullptr;
+  TypeCounts* cscan = c.weighted ? W.alloc<TypeCounts>(n) : nullptr;
+  int* g_of_node = W.alloc<int>(cap);
+  int* small_list = W.alloc<int>(cap);
+  int* failed = W.alloc<int>(cap);
+  int* failed_list = W.alloc<int>(cap);
+  double* best_bound = W.alloc<double>(cap);
+  int* lists = W.alloc<int>(2);  // small count, failed count
   unsigned char* side = W.alloc<unsigned char>(n);
   int* flags = W.alloc<int>(n);
   int* lscan = W.alloc<int>(n);
@@ -530,12 +684,16 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
   int* root_end = W.alloc<int>(4);
   size_t tmp_bytes = 0, b1 = 0, b2 = 0, b3 = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, b1, skeys, skeys2, svals, svals, n);
-  cub::DeviceScan::InclusiveScanByKey(nullptr, b2, key, boxes, pre, BoxUnion(), n);
+  cub::DeviceScan::InclusiveScanByKey(nullptr, b2, key, boxes, pre0, BoxUnion(), n);
   cub::DeviceScan::ExclusiveSum(nullptr, b3, flags, lscan, std::max(n, cap));
   tmp_bytes = std::max(b1, std::max(b2, b3));
-  size_t b4 = 0;
+  size_t b4 = 0, b5 = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, b4, tkeys, tkeys2, svals, svals, n, 0, 2);
   tmp_bytes = std::max(tmp_bytes, b4);
+  if (c.weighted) {
+    cub::DeviceScan::InclusiveScanByKey(nullptr, b5, key, onehot, cscan, CountsAdd(), n);
+    tmp_bytes = std::max(tmp_bytes, b5);
+  }
   void* tmp = W.alloc<char>(tmp_bytes);
   if (!W.ok) return fail(ctx, RTB_ERR_OUT_OF_MEMORY, "BVH build workspace");
 
@@ -574,48 +732,94 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
   k_init_keys<<<roots, 256, 0, sm>>>(key, root_start, root_end, roots);
 
   // ---- level loop
+  TypeWeights tw;
+  for (int t = 0; t < 4; ++t) tw.w[t] = c.weighted ? 1.0 + c.lambda * (c.measured[t] - 1.0) : 1.0;
+  int largest = 0;  // primitives in the level's largest node
+  for (int r = 0; r < roots; ++r) largest = std::max(largest, h_re[r] - h_rs[r]);
+  int sequential_nodes = 0;
   std::vector<int> level_begin = {0};
   int k = roots, level = 0, total_nodes = roots;
+  auto costs = [&](int certified) {
+    for (int a = 0; a < 3; ++a)
+      k_costs<<<blocks(n), 256, 0, sm>>>(P, I.a[a], N, key, level_of, level, a, n, pre_ax[a],
+                                         suf_ax[a], chains.pw[a], chains.sw[a], c.traversal,
+                                         certified, cost[a], bound[a]);
+  };
+  auto argmin = [&]() {
+    k_arg_chunk_counts<<<blocks(k), 256, 0, sm>>>(N, active, k, arg_counts,
+                                                  (unsigned long long*)best_cost, best_flat);
+    size_t tb = tmp_bytes;
+    cub::DeviceScan::InclusiveSum(tmp, tb, arg_counts, arg_ends, k, sm);
+    // chunks <= (positions / kArgChunk) + one per node; surplus blocks find no node
+    long long nb = (long long)n / kArgChunk + k + 1;
+    k_argmin_chunks<<<(unsigned)nb, 256, 0, sm>>>(N, active, k, arg_ends, cost[0], cost[1], cost[2],
+                                                  part_cost, part_flat, part_node,
+                                                  (unsigned long long*)best_cost);
+    k_argmin_flat<<<blocks(nb), 256, 0, sm>>>((int)nb, part_cost, part_flat, part_node, best_cost,
+                                              best_flat);
+  };
   while (k > 0) {
     level_begin.push_back(level_begin.back() + k);
-    // weight sums of all three axis orders first (one launch for the sequential chains)
+    const bool certify = c.weighted && largest > kSeqNodeSize;
+    // weight sums of all three axis orders first: sequential chains for the small nodes (one
+    // launch), per-type counts for the large ones
     if (c.weighted) {
       for (int a = 0; a < 3; ++a)
         k_gather_weights<<<blocks(n), 256, 0, sm>>>(P, I.a[a], n, const_cast<double*>(chains.w[a]));
-      k_weights_seq<<<blocks(6LL * 32 * k, 128), 128, 0, sm>>>(chains, N, active, k);
+      cudaMemsetAsync(lists, 0, 2 * sizeof(int), sm);
+      k_split_lists<<<blocks(k), 256, 0, sm>>>(N, active, k, small_list, lists, g_of_node);
+      k_weights_seq<<<blocks(6LL * 32 * k, 128), 128, 0, sm>>>(chains, N, small_list, k, lists);
+      if (certify) {
+        for (int a = 0; a < 3; ++a) {
+          k_type_onehot<<<blocks(n), 256, 0, sm>>>(P, I.a[a], n, onehot);
+          size_t tb = tmp_bytes;
+          cub::DeviceScan::InclusiveScanByKey(tmp, tb, key, onehot, cscan, CountsAdd(), n,
+                                              cub::Equality(), sm);
+          k_weights_counts<<<blocks(n), 256, 0, sm>>>(N, key, level_of, level, n, cscan, tw,
+                                                      chains.pw[a], chains.sw[a]);
+        }
+      }
     } else {
       k_weights_unit<<<blocks(n), 256, 0, sm>>>(N, key, level_of, level, n, chains.pw[0], chains.sw[0]);
     }
     for (int a = 0; a < 3; ++a) {
       size_t tb = tmp_bytes;
       k_gather_boxes<<<blocks(n), 256, 0, sm>>>(P, I.a[a], n, false, key, boxes, key_rev);
-      cub::DeviceScan::InclusiveScanByKey(tmp, tb, key, boxes, a == 0 ? pre0 : pre, BoxUnion(), n,
+      cub::DeviceScan::InclusiveScanByKey(tmp, tb, key, boxes, pre_ax[a], BoxUnion(), n,
                                           cub::Equality(), sm);
       k_gather_boxes<<<blocks(n), 256, 0, sm>>>(P, I.a[a], n, true, key, boxes, key_rev);
       tb = tmp_bytes;
-      cub::DeviceScan::InclusiveScanByKey(tmp, tb, key_rev, boxes, suf, BoxUnion(), n,
+      cub::DeviceScan::InclusiveScanByKey(tmp, tb, key_rev, boxes, suf_ax[a], BoxUnion(), n,
                                           cub::Equality(), sm);
-      k_costs<<<blocks(n), 256, 0, sm>>>(P, I.a[a], N, key, level_of, level, a, n,
-                                         a == 0 ? pre0 : pre, suf, chains.pw[a], chains.sw[a],
-                                         c.traversal, cost[a]);
     }
-    {
-      k_arg_chunk_counts<<<blocks(k), 256, 0, sm>>>(N, active, k, arg_counts,
-                                                    (unsigned long long*)best_cost, best_flat);
-      size_t tb = tmp_bytes;
-      cub::DeviceScan::InclusiveSum(tmp, tb, arg_counts, arg_ends, k, sm);
-      // chunks <= (positions / kArgChunk) + one per node; surplus blocks find no node
-      long long nb = (long long)n / kArgChunk + k + 1;
-      k_argmin_chunks<<<(unsigned)nb, 256, 0, sm>>>(N, active, k, arg_ends, cost[0], cost[1], cost[2],
-                                                    part_cost, part_flat, part_node,
-                                                    (unsigned long long*)best_cost);
-      k_argmin_flat<<<blocks(nb), 256, 0, sm>>>((int)nb, part_cost, part_flat, part_node, best_cost,
-                                                best_flat);
+    costs(certify ? 1 : 0);
+    argmin();
+    if (certify) {
+      // large nodes whose winner is not clear of the others' bounds: sequential weights,
+      // their costs again, and the argmin again (unchanged for every other node)
+      k_best_bound<<<blocks(k), 256, 0, sm>>>(N, active, k, best_cost, best_flat, bound[0], bound[1],
+                                              bound[2], best_bound, failed);
+      for (int a = 0; a < 3; ++a)
+        k_certify<<<blocks(n), 256, 0, sm>>>(N, key, level_of, level, a, n, g_of_node, cost[a],
+                                             bound[a], best_cost, best_flat, best_bound, failed);
+      k_failed_list<<<blocks(k), 256, 0, sm>>>(active, k, failed, failed_list, lists + 1);
+      int nfail = 0;
+      cudaMemcpyAsync(&nfail, lists + 1, 4, cudaMemcpyDeviceToHost, sm);
+      cudaError_t e = cudaStreamSynchronize(sm);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "BVH build level");
+      if (nfail > 0) {
+        k_weights_seq<<<blocks(6LL * 32 * nfail, 128), 128, 0, sm>>>(chains, N, failed_list, nfail,
+                                                                     nullptr);
+        costs(0);
+        argmin();
+        sequential_nodes += nfail;
+      }
     }
     cudaMemsetAsync(counters + 1, 0, 4, sm);
+    cudaMemsetAsync(counters + 6, 0, 4, sm);
     k_decide<<<blocks(k), 256, 0, sm>>>(P, I, N, active, k, best_cost, best_flat, pre0, c.leaf_size,
                                         counters, next_active, counters + 1, level_of, level,
-                                        counters + 2);
+                                        counters + 2, counters + 6);
     k_sides<<<blocks(n), 256, 0, sm>>>(I, N, key, level_of, level, n, side);
     for (int a = 0; a < 3; ++a) {
       k_left_flags<<<blocks(n), 256, 0, sm>>>(I.a[a], N, key, level_of, level, n, side, flags);
@@ -625,10 +829,12 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
       std::swap(I.a[a], T.a[a]);
     }
     k_update_keys<<<blocks(n), 256, 0, sm>>>(N, level_of, level, n, key);
-    int next = 0;
-    cudaMemcpyAsync(&next, counters + 1, 4, cudaMemcpyDeviceToHost, sm);
+    int next_info[6] = {0, 0, 0, 0, 0, 0};  // counters[1..6]: next count, ..., largest child
+    cudaMemcpyAsync(next_info, counters + 1, sizeof(next_info), cudaMemcpyDeviceToHost, sm);
     cudaError_t e = cudaStreamSynchronize(sm);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "BVH build level");
+    int next = next_info[0];
+    largest = next_info[5];
     if (next > 0) {
       cudaMemcpyAsync(all_nodes + total_nodes, next_active, (size_t)next * 4, cudaMemcpyDeviceToDevice, sm);
       std::swap(active, next_active);
@@ -672,7 +878,10 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
   }
   rtb_status fs = finish_build(ctx, desc, cfg, W, c, P, I, N, all_nodes, level_begin, roots, total_nodes,
                                counters, out, stats);
-  if (fs == RTB_OK && stats) stats->rotation_count = rotation_count;
+  if (fs == RTB_OK && stats) {
+    stats->rotation_count = rotation_count;
+    stats->sequential_nodes = sequential_nodes;
+  }
   return fs;
 }
 

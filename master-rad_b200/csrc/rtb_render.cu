@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(256) k_trace(DevScene S, const float* rays, in
   }
 }
 
-int g_render_blocks_per_sm[2][2] = {{0, 0}, {0, 0}};
+int g_render_blocks_per_sm[2][3] = {{0, 0, 0}, {0, 0, 0}};
 
 // Scenes whose traversal data (nodes, references, primitive records) exceed this many bytes
 // use the shared-memory stack: on the 1M-primitive scene (about 150 MB) it was 5 % faster,
@@ -315,7 +315,7 @@ constexpr long long kMaxTailItems = 1LL << 26;
 struct FramePlan {
   RenderArgs a;
   int metrics = 0;
-  int shared_stack = 0;       // k_render's SDEPTH: 0 or kSharedStackDepth
+  int shared_stack = 0;       // k_render's SDEPTH: 0, 8 or kSharedStackDepth
   long long resident = 0;     // threads of a full-occupancy grid
   long long tail_pixels = 0;  // the frame's last pixels, queued one sample per item
   long long grid = 0;
@@ -324,14 +324,16 @@ struct FramePlan {
 namespace {
 
 const void* render_kernel(int metrics, int shared_stack) {
-  if (shared_stack)
+  if (shared_stack == kSharedStackDepth)
     return metrics ? (const void*)k_render<true, kSharedStackDepth>
                    : (const void*)k_render<false, kSharedStackDepth>;
+  if (shared_stack == 8)
+    return metrics ? (const void*)k_render<true, 8> : (const void*)k_render<false, 8>;
   return metrics ? (const void*)k_render<true, 0> : (const void*)k_render<false, 0>;
 }
 
 int frame_blocks_per_sm(int metrics, int shared_stack) {
-  int& bps = g_render_blocks_per_sm[metrics][shared_stack ? 1 : 0];
+  int& bps = g_render_blocks_per_sm[metrics][shared_stack == 0 ? 0 : shared_stack == 8 ? 1 : 2];
   if (bps == 0) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, render_kernel(metrics, shared_stack), 128, 0);
     if (bps < 1) bps = 1;
@@ -385,7 +387,12 @@ rtb_status plan_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
   a.row_stride = row_stride;
   a.pixels = (long long)p->width * ((p->height - row0 + row_stride - 1) / row_stride);
   f->metrics = p->collect_metrics ? 1 : 0;
-  f->shared_stack = traversal_bytes(a.S) > kSharedStackSceneBytes ? kSharedStackDepth : 0;
+  // rtb_render_params.shared_stack_entries: 0 picks by scene size, -1 none, 8 or 16 entries
+  int se = p->shared_stack_entries;
+  if (se != 0 && se != -1 && se != 8 && se != kSharedStackDepth)
+    return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "shared_stack_entries must be 0, -1, 8 or 16");
+  f->shared_stack = se == 0 ? (traversal_bytes(a.S) > kSharedStackSceneBytes ? kSharedStackDepth : 0)
+                  : se < 0 ? 0 : se;
   f->resident = (long long)ctx->sm_count * frame_blocks_per_sm(f->metrics, f->shared_stack) * 128;
   // Tail: about four pixels per resident thread are split into single samples.
   long long tail_pixels = std::min<long long>(a.pixels, (long long)(RTB_TAIL_FACTOR * f->resident));
@@ -408,11 +415,16 @@ void bind_frame(FramePlan* f, unsigned long long* queue, float* tail, int* abort
 
 int launch_frame(const FramePlan* f, cudaStream_t stream) {
   const RenderArgs& a = f->a;
-  if (f->shared_stack) {
+  if (f->shared_stack == kSharedStackDepth) {
     if (f->metrics)
       k_render<true, kSharedStackDepth><<<(unsigned)f->grid, 128, 0, stream>>>(a);
     else
       k_render<false, kSharedStackDepth><<<(unsigned)f->grid, 128, 0, stream>>>(a);
+  } else if (f->shared_stack == 8) {
+    if (f->metrics)
+      k_render<true, 8><<<(unsigned)f->grid, 128, 0, stream>>>(a);
+    else
+      k_render<false, 8><<<(unsigned)f->grid, 128, 0, stream>>>(a);
   } else {
     if (f->metrics)
       k_render<true, 0><<<(unsigned)f->grid, 128, 0, stream>>>(a);

@@ -73,7 +73,7 @@ class RenderParams(C.Structure):
     _fields_ = [("width", C.c_int), ("height", C.c_int), ("samples_per_frame", C.c_int),
                 ("max_depth", C.c_int), ("frame_index", C.c_int),
                 ("frame_seed", C.c_ulonglong), ("use_bvh", C.c_int),
-                ("collect_metrics", C.c_int), ("block_size", C.c_int)]
+                ("collect_metrics", C.c_int), ("shared_stack_entries", C.c_int)]
 
 
 class FrameStats(C.Structure):
