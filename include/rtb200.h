@@ -228,6 +228,13 @@ RTB_API rtb_status rtb_render_backward(rtb_context* ctx, rtb_scene* scene, const
                                        const rtb_render_params* params, const float* adjoint_device,
                                        float* grad_albedo_device, float* grad_emission_device,
                                        void* stream);
+/* rtb_render_backward with host buffers (dLoss/dImage in, 3 floats per pixel; the two
+ * gradient tables out, 3 floats per material each), staged through the context's device
+ * buffers; returns when the gradients are written, or RTB_ERR_WATCHDOG after an abort.  The
+ * entry a caller without CUDA memory of its own binds (the Java forward/backward Function). */
+RTB_API rtb_status rtb_render_backward_sample(rtb_context* ctx, rtb_scene* scene, const rtb_camera* camera,
+                                              const rtb_render_params* params, const float* adjoint,
+                                              float* grad_albedo, float* grad_emission);
 
 /* ---- batched rendering (no counterpart in the reference, which renders one scene per
  *      renderSample call) ----
@@ -248,6 +255,14 @@ typedef struct {
   int branches;               /* 0: one shared-queue kernel over all jobs; 1..4: each job
                                  its own persistent frame, the frames spread round-robin
                                  over this many concurrent graph branches */
+  int shared_stack_entries;   /* traversal-stack depth kept in shared memory by the jobs'
+                                 frames (branches > 0): 0 keeps each job's own
+                                 rtb_render_params value, else -1, 8 or 16 for every job */
+  int tail_pixels_per_thread; /* queue granularity at the end of a frame (or of the
+                                 shared-queue batch): this many pixels per resident thread
+                                 are queued one sample per item instead of one pixel per
+                                 item; 0: the default (4 for frames, 2 for the shared
+                                 queue), else 1..16 */
 } rtb_batch_tuning;
 
 typedef struct rtb_batch rtb_batch;
@@ -257,8 +272,12 @@ RTB_API rtb_status rtb_batch_create(rtb_context* ctx, const rtb_batch_job* jobs,
                                     const rtb_batch_tuning* tuning, rtb_batch** out);
 /* Replays the batch's graph on `stream` (NULL: the context stream); returns once queued. */
 RTB_API rtb_status rtb_batch_render(rtb_context* ctx, rtb_batch* batch, void* stream);
-/* Times every candidate tuning on the batch itself (`repeats` timed runs each after a
- * warm-up run), keeps the fastest, re-captures the graph and reports it. */
+/* Times candidate tunings on the batch itself (`repeats` timed runs each after a warm-up
+ * run) and keeps the fastest: first every kernel form (shared queue at 64/128/256 threads,
+ * frames over 1/2/4 branches) in both job orders, then, around the best, the end-of-frame
+ * queue granularity (1, 2, 4, 8 pixels per thread at one sample per item) and, for frames,
+ * the shared-memory stack depth (none, 8, 16 entries, by scene size); re-captures the graph
+ * and reports the choice. */
 RTB_API rtb_status rtb_batch_autotune(rtb_context* ctx, rtb_batch* batch, int repeats,
                                       rtb_batch_tuning* best, double* best_ms);
 RTB_API rtb_status rtb_batch_destroy(rtb_context* ctx, rtb_batch* batch);

@@ -285,19 +285,18 @@ rtb_status rtb_scene_set_materials(rtb_context* ctx, rtb_scene* scene, const flo
   return e == cudaSuccess ? RTB_OK : cuda_fail(ctx, e, "material update");
 }
 
-rtb_status rtb_render_backward(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
-                               const rtb_render_params* p, const float* adjoint_device,
-                               float* grad_albedo_device, float* grad_emission_device, void* stream) {
-  if (!ctx) return RTB_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  cudaSetDevice(ctx->device);
+// The backward launch; the caller holds the context lock with its device current.
+static rtb_status render_backward(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
+                                  const rtb_render_params* p, const float* adjoint_device,
+                                  float* grad_albedo_device, float* grad_emission_device,
+                                  cudaStream_t stream) {
   if (!scene || !cam || !p || !adjoint_device || !grad_albedo_device || !grad_emission_device)
     return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "null argument");
   if (p->width < 1 || p->height < 1 || p->samples_per_frame < 1)
     return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "image size and samples must be positive");
   if (p->max_depth < 0 || p->max_depth > kMaxVertices)
     return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "GPU full-path depth must be in [0, 32]");
-  cudaStream_t sm = stream ? (cudaStream_t)stream : ctx->stream;
+  cudaStream_t sm = stream ? stream : ctx->stream;
   ctx_acquire(ctx, sm);
   AdjointArgs a;
   a.S = scene->dev;
@@ -333,6 +332,52 @@ rtb_status rtb_render_backward(rtb_context* ctx, rtb_scene* scene, const rtb_cam
   ctx_release(ctx, sm);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint launch");
+  return RTB_OK;
+}
+
+rtb_status rtb_render_backward(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
+                               const rtb_render_params* p, const float* adjoint_device,
+                               float* grad_albedo_device, float* grad_emission_device, void* stream) {
+  if (!ctx) return RTB_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  cudaSetDevice(ctx->device);
+  return render_backward(ctx, scene, cam, p, adjoint_device, grad_albedo_device,
+                         grad_emission_device, (cudaStream_t)stream);
+}
+
+rtb_status rtb_render_backward_sample(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
+                                      const rtb_render_params* p, const float* adjoint,
+                                      float* grad_albedo, float* grad_emission) {
+  if (!ctx) return RTB_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  cudaSetDevice(ctx->device);
+  if (!scene || !p || !adjoint || !grad_albedo || !grad_emission)
+    return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "null argument");
+  if (p->width < 1 || p->height < 1)
+    return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "image size and samples must be positive");
+  size_t img = (size_t)p->width * p->height * 3 * sizeof(float);
+  size_t grads = (size_t)scene->dev.material_count * 3 * sizeof(float);
+  size_t img_pad = (img + 255) & ~(size_t)255, grads_pad = (grads + 255) & ~(size_t)255;
+  char* d = (char*)stage(ctx, img_pad + 2 * grads_pad);
+  if (!d) return fail(ctx, RTB_ERR_OUT_OF_MEMORY, "adjoint staging");
+  float* d_adj = (float*)d;
+  float* d_ga = (float*)(d + img_pad);
+  float* d_ge = (float*)(d + img_pad + grads_pad);
+  cudaStream_t sm = ctx->stream;
+  ctx_acquire(ctx, sm);
+  cudaMemcpyAsync(d_adj, adjoint, img, cudaMemcpyHostToDevice, sm);
+  ctx_release(ctx, sm);
+  rtb_status s = render_backward(ctx, scene, cam, p, d_adj, d_ga, d_ge, sm);
+  if (s != RTB_OK) return s;
+  ctx_acquire(ctx, sm);
+  cudaMemcpyAsync(grad_albedo, d_ga, grads, cudaMemcpyDeviceToHost, sm);
+  cudaMemcpyAsync(grad_emission, d_ge, grads, cudaMemcpyDeviceToHost, sm);
+  ctx_release(ctx, sm);
+  cudaError_t e = cudaStreamSynchronize(sm);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint");
+  int aborted = 0;
+  cudaMemcpy(&aborted, ctx->d_abort + 2, sizeof(int), cudaMemcpyDeviceToHost);
+  if (aborted) return fail(ctx, RTB_ERR_WATCHDOG, "backward pass aborted on request");
   return RTB_OK;
 }
 

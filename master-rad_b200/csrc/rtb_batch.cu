@@ -344,8 +344,10 @@ rtb_status plan_frames(rtb_context* ctx, rtb_batch* B, const std::vector<int>& o
     const rtb_batch_job& j = B->jobs[order[i]];
     rtb_render_params p = j.params;
     p.collect_metrics = 0;
+    if (B->tuning.shared_stack_entries != 0) p.shared_stack_entries = B->tuning.shared_stack_entries;
     FramePlan* f = new_frame_plan();
-    rtb_status s = plan_frame(ctx, j.scene, &j.camera, &p, j.rgb_device, f);
+    rtb_status s = plan_frame(ctx, j.scene, &j.camera, &p, j.rgb_device, f, 0, 1,
+                              B->tuning.tail_pixels_per_thread);
     if (s != RTB_OK) {
       delete_frame_plan(f);
       free_frames(B);
@@ -403,7 +405,8 @@ rtb_status upload_jobs(rtb_context* ctx, rtb_batch* B) {
   // Tail: the last jobs' last pixels, about two per resident thread, as single samples.
   std::vector<long long> tail(order.size(), 0);
   {
-    long long want = 2LL * ctx->sm_count * blocks_per_sm(B->tuning.threads_per_block) *
+    long long per_thread = B->tuning.tail_pixels_per_thread > 0 ? B->tuning.tail_pixels_per_thread : 2;
+    long long want = per_thread * ctx->sm_count * blocks_per_sm(B->tuning.threads_per_block) *
                      B->tuning.threads_per_block;
     long long items_left = kMaxBatchTailItems;
     for (size_t k = order.size(); k-- > 0 && want > 0;) {
@@ -542,6 +545,13 @@ rtb_status rtb_batch_create(rtb_context* ctx, const rtb_batch_job* jobs, int job
     delete B;
     return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "branches must be in [0, 4]");
   }
+  int se = B->tuning.shared_stack_entries;
+  if ((se != 0 && se != -1 && se != 8 && se != 16) || B->tuning.tail_pixels_per_thread < 0 ||
+      B->tuning.tail_pixels_per_thread > 16) {
+    delete B;
+    return fail(ctx, RTB_ERR_INVALID_ARGUMENT,
+                "shared_stack_entries must be 0, -1, 8 or 16 and tail_pixels_per_thread in [0, 16]");
+  }
   cudaError_t e = cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming);
   for (int b = 0; b < kMaxBranches && e == cudaSuccess; ++b) {
     e = cudaStreamCreateWithFlags(&B->branch[b], cudaStreamNonBlocking);
@@ -580,44 +590,66 @@ rtb_status rtb_batch_autotune(rtb_context* ctx, rtb_batch* B, int repeats, rtb_b
   std::lock_guard<std::mutex> lock(ctx->mu);
   cudaSetDevice(ctx->device);
   if (repeats < 1) repeats = 1;
-  // Candidates: the shared-queue kernel at 64/128/256 threads, and per-job frames over
-  // 1/2/4 graph branches; each in the caller's order and most expensive first.
-  std::vector<rtb_batch_tuning> cands;
-  for (int order = 0; order < 2; ++order) {
-    for (int t : {64, 128, 256}) cands.push_back({t, order, 0});
-    for (int k : {1, 2, 4}) cands.push_back({128, order, k});
-  }
   double best_time = 1e300;
   rtb_batch_tuning pick = B->tuning;
   cudaStream_t sm = ctx->stream;
   ctx_acquire(ctx, sm);
   rtb_status s = RTB_OK;
-  for (const rtb_batch_tuning& c : cands) {
-    B->tuning = c;
-    s = upload_jobs(ctx, B);
-    if (s != RTB_OK) break;
-    double total = 0.0;
-    for (int r = 0; r <= repeats && s == RTB_OK; ++r) {  // first run warms up
-      arm_abort(ctx, sm);
-      cudaEventRecord(ctx->ev0, sm);
-      s = enqueue(ctx, B, sm);
-      if (s != RTB_OK) break;
-      cudaEventRecord(ctx->ev1, sm);
-      cudaError_t e = cudaEventSynchronize(ctx->ev1);
-      if (e != cudaSuccess) {
-        s = cuda_fail(ctx, e, "batch autotune");
-        break;
+  auto try_all = [&](const std::vector<rtb_batch_tuning>& cands) {
+    for (const rtb_batch_tuning& c : cands) {
+      B->tuning = c;
+      s = upload_jobs(ctx, B);
+      if (s != RTB_OK) return;
+      double total = 0.0;
+      for (int r = 0; r <= repeats && s == RTB_OK; ++r) {  // first run warms up
+        arm_abort(ctx, sm);
+        cudaEventRecord(ctx->ev0, sm);
+        s = enqueue(ctx, B, sm);
+        if (s != RTB_OK) return;
+        cudaEventRecord(ctx->ev1, sm);
+        cudaError_t e = cudaEventSynchronize(ctx->ev1);
+        if (e != cudaSuccess) {
+          s = cuda_fail(ctx, e, "batch autotune");
+          return;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        if (r > 0) total += ms;
       }
-      float ms = 0.0f;
-      cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-      if (r > 0) total += ms;
+      double mean = total / repeats;
+      if (mean < best_time) {
+        best_time = mean;
+        pick = c;
+      }
     }
-    if (s != RTB_OK) break;
-    double mean = total / repeats;
-    if (mean < best_time) {
-      best_time = mean;
-      pick = c;
+  };
+  // Stage 1: the kernel form -- the shared-queue kernel at 64/128/256 threads, or per-job
+  // frames over 1/2/4 graph branches -- each in the caller's order and most expensive first.
+  std::vector<rtb_batch_tuning> cands;
+  for (int order = 0; order < 2; ++order) {
+    for (int t : {64, 128, 256}) cands.push_back({t, order, 0, 0, 0});
+    for (int k : {1, 2, 4}) cands.push_back({128, order, k, 0, 0});
+  }
+  try_all(cands);
+  // Stage 2: queue granularity at the end of the frames (or of the shared queue).
+  if (s == RTB_OK) {
+    cands.clear();
+    for (int t : {1, 2, 4, 8}) {
+      rtb_batch_tuning c = pick;
+      c.tail_pixels_per_thread = t;
+      cands.push_back(c);
     }
+    try_all(cands);
+  }
+  // Stage 3: for per-job frames, the traversal-stack entries kept in shared memory.
+  if (s == RTB_OK && pick.branches > 0) {
+    cands.clear();
+    for (int e : {-1, 8, 16}) {
+      rtb_batch_tuning c = pick;
+      c.shared_stack_entries = e;
+      cands.push_back(c);
+    }
+    try_all(cands);
   }
   ctx_release(ctx, sm);
   B->tuning = pick;

@@ -380,11 +380,270 @@ __global__ void k_argmin_flat(int blocks_total, const double* part_cost, const l
   if (part_cost[b] == best_cost[g]) atomicMin(best_flat + g, part_flat[b]);
 }
 
+// ---- whole subtrees of at most kSubtreeSize primitives, one warp each
+//
+// The recursion of BvhBuildState.build (GpuScene.java:1424-1447) below such a node runs in
+// one warp, depth first, with the node's three axis orders in shared memory: per node and
+// axis the suffix boxes and weights (weights summed one by one in the reference's order,
+// the same additions as its loop), then the prefix pass evaluating every split's cost in the
+// reference's expression order, the first minimum over (axis, position), the leaf rule in
+// the node's current order, and a stable partition of the other two axis orders.  Every
+// number is the one the level loop would compute for the same node; the subtree only saves
+// the per-level passes over all primitives (scans, gathers, argmin blocks) that dominate
+// the deep levels.
+constexpr int kSubtreeSize = kSeqNodeSize;
+constexpr int kSubtreeWarps = 2;
+
+struct SubtreeSmem {
+  int idx[3][kSubtreeSize];
+  Box sbox[kSubtreeSize];
+  double sw[kSubtreeSize];
+  int tmp[kSubtreeSize];
+  int stack[kSubtreeSize];
+};
+
+__device__ __forceinline__ Box empty_box() {
+  Box b;
+  for (int k = 0; k < 3; ++k) {
+    b.mn[k] = CUDART_INF_F;
+    b.mx[k] = -CUDART_INF_F;
+  }
+  return b;
+}
+
+__device__ __forceinline__ Box prim_box(const Prims& P, int p) {
+  Box b;
+  for (int k = 0; k < 3; ++k) {
+    b.mn[k] = P.lo[k][p];
+    b.mx[k] = P.hi[k][p];
+  }
+  return b;
+}
+
+// Inclusive union over lanes 0..lane (min / max are exact in any order).
+__device__ __forceinline__ Box warp_union_scan(Box b, int lane) {
+  for (int off = 1; off < 32; off <<= 1) {
+    Box o;
+    for (int k = 0; k < 3; ++k) {
+      o.mn[k] = __shfl_up_sync(0xFFFFFFFFu, b.mn[k], off);
+      o.mx[k] = __shfl_up_sync(0xFFFFFFFFu, b.mx[k], off);
+    }
+    if (lane >= off) b = BoxUnion()(b, o);
+  }
+  return b;
+}
+
+__device__ __forceinline__ Box warp_bcast(const Box& b, int src) {
+  Box r;
+  for (int k = 0; k < 3; ++k) {
+    r.mn[k] = __shfl_sync(0xFFFFFFFFu, b.mn[k], src);
+    r.mx[k] = __shfl_sync(0xFFFFFFFFu, b.mx[k], src);
+  }
+  return r;
+}
+
+// Running sums of the 32 lanes' weights in lane order, continuing `acc`: lane q gets
+// acc + w_0 + ... + w_q added one by one (only the first `valid` lanes take part).
+__device__ __forceinline__ double warp_sequential_sum(double w, double& acc, int lane, int valid) {
+  double mine = 0.0;
+  for (int q = 0; q < valid; ++q) {
+    double v = __shfl_sync(0xFFFFFFFFu, w, q);
+    acc = acc + v;
+    if (q == lane) mine = acc;
+  }
+  return mine;
+}
+
+__global__ void __launch_bounds__(32 * kSubtreeWarps) k_subtrees(
+    const Prims P, IdxSet I, Nodes N, const int* roots, const int* root_count, int leaf_size,
+    double traversal, int* node_counter, int* stats, unsigned char* side) {
+  __shared__ SubtreeSmem smem[kSubtreeWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = blockIdx.x * kSubtreeWarps + warp;
+  if (g >= *root_count) return;
+  SubtreeSmem& sm = smem[warp];
+  const int root = roots[g];
+  const int rs = N.start[root], re = N.end[root], M = re - rs;
+  for (int a = 0; a < 3; ++a)
+    for (int i = lane; i < M; i += 32) sm.idx[a][i] = I.a[a][rs + i];
+  int sp = 0;
+  if (lane == 0) sm.stack[0] = root;
+  sp = 1;
+  __syncwarp();
+  while (sp > 0) {
+    const int node = sm.stack[--sp];
+    __syncwarp();
+    const int s = N.start[node], e = N.end[node], m = e - s, lo = s - rs;
+    const int oa = N.order_axis[node];
+    // node bounds
+    Box nb = empty_box();
+    for (int i = lane; i < m; i += 32) nb = BoxUnion()(nb, prim_box(P, sm.idx[0][lo + i]));
+    for (int off = 16; off > 0; off >>= 1) {
+      Box o;
+      for (int k = 0; k < 3; ++k) {
+        o.mn[k] = __shfl_xor_sync(0xFFFFFFFFu, nb.mn[k], off);
+        o.mx[k] = __shfl_xor_sync(0xFFFFFFFFu, nb.mx[k], off);
+      }
+      nb = BoxUnion()(nb, o);
+    }
+    const double node_a = surface_area(nb) * traversal;
+    double best = CUDART_INF;
+    long long best_flat = 0x7FFFFFFFFFFFFFFFLL;
+    if (m > 1) {
+      for (int a = 0; a < 3; ++a) {
+        const int* ix = sm.idx[a] + lo;
+        double ext = P.cen[a][ix[m - 1]] - P.cen[a][ix[0]];
+        if (!(ext > 1.0e-12)) continue;
+        // suffix boxes and weights, from the last position down (GpuScene.java:1476-1480)
+        Box carry = empty_box();
+        double acc = 0.0;
+        for (int base = 0; base < m; base += 32) {
+          int q = m - 1 - (base + lane);
+          int valid = min(32, m - base);
+          Box b = q >= 0 ? prim_box(P, ix[q]) : empty_box();
+          double w = q >= 0 ? P.w[ix[q]] : 0.0;
+          b = BoxUnion()(warp_union_scan(b, lane), carry);
+          double sw = warp_sequential_sum(w, acc, lane, valid);
+          if (q >= 0) {
+            sm.sbox[lo + q] = b;
+            sm.sw[lo + q] = sw;
+          }
+          carry = warp_bcast(b, 31);
+        }
+        __syncwarp();
+        // prefix pass and the cost of putting local positions [0, i) left (1470-1475, 1482-1485)
+        carry = empty_box();
+        acc = 0.0;
+        for (int base = 0; base < m; base += 32) {
+          int li = base + lane;
+          int valid = min(32, m - base);
+          Box b = li < m ? prim_box(P, ix[li]) : empty_box();
+          double w = li < m ? P.w[ix[li]] : 0.0;
+          b = BoxUnion()(warp_union_scan(b, lane), carry);
+          double pw = warp_sequential_sum(w, acc, lane, valid);
+          int i = li + 1;  // split after li
+          if (i < m) {
+            double bl = surface_area(b) * pw;
+            double d = surface_area(sm.sbox[lo + i]) * sm.sw[lo + i];
+            double c = (node_a + bl) + d;
+            long long flat = (long long)a * m + i;
+            if (c < best || (c == best && flat < best_flat)) {
+              best = c;
+              best_flat = flat;
+            }
+          }
+          carry = warp_bcast(b, 31);
+        }
+        __syncwarp();
+      }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      double oc = __shfl_xor_sync(0xFFFFFFFFu, best, off);
+      long long of = __shfl_xor_sync(0xFFFFFFFFu, best_flat, off);
+      if (oc < best || (oc == best && of < best_flat)) {
+        best = oc;
+        best_flat = of;
+      }
+    }
+    // leaf rule (GpuScene.java:1435-1441), the weight sum in the node's current order
+    bool leaf = m == 1 || best == CUDART_INF;
+    if (!leaf && m <= leaf_size) {
+      double wsum = 0.0;
+      for (int j = 0; j < m; ++j) wsum = wsum + P.w[oa < 0 ? s + j : sm.idx[oa][lo + j]];
+      if (!(best < surface_area(nb) * wsum)) leaf = true;
+    }
+    if (lane == 0) {
+      N.bounds[node] = nb;
+      N.split_axis[node] = -1;
+    }
+    if (leaf) {
+      if (lane == 0) {
+        N.leaf[node] = 1;
+        atomicAdd(stats + 0, 1);
+        atomicMin(stats + 1, m);
+        atomicMax(stats + 2, m);
+        atomicMax(stats + 3, N.depth[node]);
+      }
+      __syncwarp();
+      continue;
+    }
+    const int axis = (int)(best_flat / m), pos = (int)(best_flat % m);
+    int l = 0;
+    if (lane == 0) {
+      l = atomicAdd(node_counter, 2);
+      int r = l + 1;
+      N.leaf[node] = 0;
+      N.left[node] = l;
+      N.right[node] = r;
+      N.split_axis[node] = axis;
+      N.split_pos[node] = pos;
+      N.start[l] = s;
+      N.end[l] = s + pos;
+      N.start[r] = s + pos;
+      N.end[r] = e;
+      N.order_axis[l] = N.order_axis[r] = axis;
+      N.depth[l] = N.depth[r] = N.depth[node] + 1;
+      N.leaf[l] = N.leaf[r] = 0;
+      atomicMax(stats + 3, N.depth[node] + 1);
+    }
+    l = __shfl_sync(0xFFFFFFFFu, l, 0);
+    // stable partition of the other two axis orders by side
+    for (int i = lane; i < m; i += 32) side[sm.idx[axis][lo + i]] = i >= pos ? 1 : 0;
+    __syncwarp();
+    for (int a = 0; a < 3; ++a) {
+      if (a == axis) continue;
+      int nl = 0;
+      for (int base = 0; base < m; base += 32) {
+        int li = base + lane;
+        bool in = li < m;
+        int p = in ? sm.idx[a][lo + li] : 0;
+        bool left = in && side[p] == 0;
+        unsigned bal = __ballot_sync(0xFFFFFFFFu, left);
+        if (left) sm.tmp[lo + nl + __popc(bal & ((1u << lane) - 1u))] = p;
+        nl += __popc(bal);
+      }
+      int nr = 0;
+      for (int base = 0; base < m; base += 32) {
+        int li = base + lane;
+        bool in = li < m;
+        int p = in ? sm.idx[a][lo + li] : 0;
+        bool right = in && side[p] != 0;
+        unsigned bal = __ballot_sync(0xFFFFFFFFu, right);
+        if (right) sm.tmp[lo + pos + nr + __popc(bal & ((1u << lane) - 1u))] = p;
+        nr += __popc(bal);
+      }
+      __syncwarp();
+      for (int i = lane; i < m; i += 32) sm.idx[a][lo + i] = sm.tmp[lo + i];
+      __syncwarp();
+    }
+    if (lane == 0) {
+      sm.stack[sp] = l + 1;
+      sm.stack[sp + 1] = l;
+    }
+    sp += 2;
+    __syncwarp();
+  }
+  for (int a = 0; a < 3; ++a)
+    for (int i = lane; i < M; i += 32) I.a[a][rs + i] = sm.idx[a][i];
+}
+
+// Nodes per depth, then all nodes listed level by level (the finishing passes walk them).
+__global__ void k_depth_hist(const Nodes N, int count, int* hist) {
+  int node = blockIdx.x * blockDim.x + threadIdx.x;
+  if (node < count) atomicAdd(hist + N.depth[node], 1);
+}
+
+__global__ void k_depth_scatter(const Nodes N, int count, int* cursor, int* all_nodes) {
+  int node = blockIdx.x * blockDim.x + threadIdx.x;
+  if (node < count) all_nodes[atomicAdd(cursor + N.depth[node], 1)] = node;
+}
+
 // Leaf-or-split decision per active node (GpuScene.java:1424-1447).
 __global__ void k_decide(const Prims P, IdxSet I, Nodes N, const int* active, int k,
                          const double* best_cost, const long long* best_flat, const Box* pre0,
                          int leaf_size, int* node_counter, int* next_active, int* next_count,
-                         int* level_of, int level, int* stats, int* largest_child) {
+                         int* level_of, int level, int* stats, int* largest_child, int* small_roots,
+                         int* small_count) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= k) return;
   int node = active[g];
@@ -425,12 +684,20 @@ __global__ void k_decide(const Prims P, IdxSet I, Nodes N, const int* active, in
   N.order_axis[l] = N.order_axis[r] = axis;
   N.depth[l] = N.depth[r] = N.depth[node] + 1;
   N.leaf[l] = N.leaf[r] = 0;
-  level_of[l] = level_of[r] = level + 1;
   atomicMax(stats + 3, N.depth[node] + 1);
-  int q = atomicAdd(next_count, 2);
-  next_active[q] = l;
-  next_active[q + 1] = r;
-  atomicMax(largest_child, max(pos, n - pos));
+  // children of at most kSubtreeSize primitives leave the level loop: k_subtrees builds
+  // their whole subtrees later (level_of -1 keeps the level kernels off their positions)
+  int sizes[2] = {pos, n - pos}, kids[2] = {l, r};
+  for (int h = 0; h < 2; ++h) {
+    if (sizes[h] <= kSubtreeSize) {
+      level_of[kids[h]] = -1;
+      small_roots[atomicAdd(small_count, 1)] = kids[h];
+    } else {
+      level_of[kids[h]] = level + 1;
+      next_active[atomicAdd(next_count, 1)] = kids[h];
+      atomicMax(largest_child, sizes[h]);
+    }
+  }
 }
 
 __global__ void k_sides(IdxSet I, const Nodes N, const int* key, const int* level_of, int level, int n,
@@ -660,6 +927,8 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
   int* failed_list = W.alloc<int>(cap);
   double* best_bound = W.alloc<double>(cap);
   int* lists = W.alloc<int>(2);  // small count, failed count
+  int* sub_roots = W.alloc<int>(cap);  // nodes whose subtrees k_subtrees builds
+  int* depth_hist = W.alloc<int>(cap + 1);
   unsigned char* side = W.alloc<unsigned char>(n);
   int* flags = W.alloc<int>(n);
   int* lscan = W.alloc<int>(n);
@@ -716,29 +985,37 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
   // ---- roots
   int h_rs[4], h_re[4];
   int roots = root_ranges(c, per_type, h_rs, h_re);
-  std::vector<int> h_init(roots);
-  for (int r = 0; r < roots; ++r) h_init[r] = r;
   int h_counters[8] = {roots, 0, 0, 0x7FFFFFFF, 0, 0, 0, 0};
   cudaMemcpyAsync(root_start, h_rs, roots * 4, cudaMemcpyHostToDevice, sm);
   cudaMemcpyAsync(root_end, h_re, roots * 4, cudaMemcpyHostToDevice, sm);
   cudaMemcpyAsync(N.start, h_rs, roots * 4, cudaMemcpyHostToDevice, sm);
   cudaMemcpyAsync(N.end, h_re, roots * 4, cudaMemcpyHostToDevice, sm);
-  cudaMemcpyAsync(active, h_init.data(), roots * 4, cudaMemcpyHostToDevice, sm);
-  cudaMemcpyAsync(all_nodes, h_init.data(), roots * 4, cudaMemcpyHostToDevice, sm);
+  // roots of at most kSubtreeSize primitives go straight to the subtree kernel
+  std::vector<int> h_big, h_small, h_level(roots);
+  for (int r = 0; r < roots; ++r) {
+    bool small = h_re[r] - h_rs[r] <= kSubtreeSize;
+    (small ? h_small : h_big).push_back(r);
+    h_level[r] = small ? -1 : 0;
+  }
+  h_counters[7] = (int)h_small.size();
+  if (!h_big.empty())
+    cudaMemcpyAsync(active, h_big.data(), h_big.size() * 4, cudaMemcpyHostToDevice, sm);
+  if (!h_small.empty())
+    cudaMemcpyAsync(sub_roots, h_small.data(), h_small.size() * 4, cudaMemcpyHostToDevice, sm);
   cudaMemcpyAsync(counters, h_counters, sizeof(h_counters), cudaMemcpyHostToDevice, sm);
   cudaMemsetAsync(N.order_axis, 0xFF, (size_t)roots * 4, sm);  // -1: input order
   cudaMemsetAsync(N.depth, 0, (size_t)roots * 4, sm);
-  cudaMemsetAsync(level_of, 0, (size_t)roots * 4, sm);
+  cudaMemcpyAsync(level_of, h_level.data(), roots * 4, cudaMemcpyHostToDevice, sm);
   k_init_keys<<<roots, 256, 0, sm>>>(key, root_start, root_end, roots);
 
   // ---- level loop
   TypeWeights tw;
   for (int t = 0; t < 4; ++t) tw.w[t] = c.weighted ? 1.0 + c.lambda * (c.measured[t] - 1.0) : 1.0;
   int largest = 0;  // primitives in the level's largest node
-  for (int r = 0; r < roots; ++r) largest = std::max(largest, h_re[r] - h_rs[r]);
+  for (int r : h_big) largest = std::max(largest, h_re[r] - h_rs[r]);
   int sequential_nodes = 0;
   std::vector<int> level_begin = {0};
-  int k = roots, level = 0, total_nodes = roots;
+  int k = (int)h_big.size(), level = 0, total_nodes = roots;
   auto costs = [&](int certified) {
     for (int a = 0; a < 3; ++a)
       k_costs<<<blocks(n), 256, 0, sm>>>(P, I.a[a], N, key, level_of, level, a, n, pre_ax[a],
@@ -759,7 +1036,6 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
                                               best_flat);
   };
   while (k > 0) {
-    level_begin.push_back(level_begin.back() + k);
     const bool certify = c.weighted && largest > kSeqNodeSize;
     // weight sums of all three axis orders first: sequential chains for the small nodes (one
     // launch), per-type counts for the large ones
@@ -819,7 +1095,7 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
     cudaMemsetAsync(counters + 6, 0, 4, sm);
     k_decide<<<blocks(k), 256, 0, sm>>>(P, I, N, active, k, best_cost, best_flat, pre0, c.leaf_size,
                                         counters, next_active, counters + 1, level_of, level,
-                                        counters + 2, counters + 6);
+                                        counters + 2, counters + 6, sub_roots, counters + 7);
     k_sides<<<blocks(n), 256, 0, sm>>>(I, N, key, level_of, level, n, side);
     for (int a = 0; a < 3; ++a) {
       k_left_flags<<<blocks(n), 256, 0, sm>>>(I.a[a], N, key, level_of, level, n, side, flags);
@@ -835,13 +1111,37 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
     if (e != cudaSuccess) return cuda_fail(ctx, e, "BVH build level");
     int next = next_info[0];
     largest = next_info[5];
-    if (next > 0) {
-      cudaMemcpyAsync(all_nodes + total_nodes, next_active, (size_t)next * 4, cudaMemcpyDeviceToDevice, sm);
-      std::swap(active, next_active);
-    }
-    total_nodes += next;
+    if (next > 0) std::swap(active, next_active);
     k = next;
     level++;
+  }
+  // ---- the subtrees below the level loop, then every node listed by depth
+  {
+    int h[8];
+    cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, sm);
+    cudaError_t e = cudaStreamSynchronize(sm);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "BVH build levels");
+    if (h[7] > 0)
+      k_subtrees<<<(unsigned)((h[7] + kSubtreeWarps - 1) / kSubtreeWarps), 32 * kSubtreeWarps, 0, sm>>>(
+          P, I, N, sub_roots, counters + 7, c.leaf_size, c.traversal, counters, counters + 2, side);
+    cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, sm);
+    e = cudaStreamSynchronize(sm);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "BVH subtrees");
+    total_nodes = h[0];
+    int depths = h[5] + 1;
+    if (total_nodes < 1 || total_nodes > cap || depths < 1 || depths > cap)
+      return fail(ctx, RTB_ERR_DEVICE_CHECK, "BVH node count out of range");
+    cudaMemsetAsync(depth_hist, 0, (size_t)depths * 4, sm);
+    k_depth_hist<<<blocks(total_nodes), 256, 0, sm>>>(N, total_nodes, depth_hist);
+    std::vector<int> hist(depths);
+    cudaMemcpyAsync(hist.data(), depth_hist, (size_t)depths * 4, cudaMemcpyDeviceToHost, sm);
+    e = cudaStreamSynchronize(sm);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "BVH depth histogram");
+    level_begin.assign(1, 0);
+    for (int d = 0; d < depths; ++d) level_begin.push_back(level_begin.back() + hist[d]);
+    cudaMemcpyAsync(depth_hist, level_begin.data(), (size_t)depths * 4, cudaMemcpyHostToDevice, sm);
+    k_depth_scatter<<<blocks(total_nodes), 256, 0, sm>>>(N, total_nodes, depth_hist, all_nodes);
   }
   int rotation_count = 0;
   if (rotate) {

@@ -43,6 +43,10 @@ constexpr float kEps = 1e-4f;          // K:12
 constexpr int kTypeShift = 30;
 constexpr int kIndexMask = 0x3FFFFFFF;  // K:20
 constexpr int kStackSize = 64;          // covers every tree depth the builders produce
+// Leaf tests wait until at most this many lanes of the warp can still walk the tree
+// (measured on the 10k and 1M scenes: 4 was best of 0/4/8/12/16, 2 % above testing each
+// node's leaves at once).
+constexpr int kLeafPostponeLanes = 4;
 
 enum PrimType { kSphere = 0, kBox = 1, kAffineSphere = 2, kAffineBox = 3, kPlane = 4 };
 
@@ -479,9 +483,11 @@ __device__ __noinline__ void test_all_primitives(const DevScene& S, float3 o, fl
 //
 // Warp-cooperative: all 32 lanes of the warp call it together (lanes without a ray pass
 // active = false).  The traversal loop is warp-uniform -- each iteration every lane that
-// still has work processes one node: it tests both child boxes, then tests the primitives
-// of the (at most two) leaf children in one loop, then picks the next interior node -- and
-// the loop condition is a warp vote, so divergent lanes reconverge once per node.  Every lane
+// still walks processes one node: it tests both child boxes, records the (at most two)
+// leaf children it reached, then picks the next interior node; once at most
+// kLeafPostponeLanes lanes can still walk, the recorded leaves of all lanes are tested
+// together -- and the loop condition is a warp vote, so divergent lanes reconverge once per
+// node.  Every lane
 // takes part in the votes, also where lanes hold different scenes and only some of them
 // have a tree (the batch kernel's lanes may belong to different jobs).
 //
@@ -508,8 +514,29 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
     // A tree visits each node at most once per ray; the cap only matters for malformed
     // (cyclic) caller-supplied trees, which then take the exhaustive path.
     int budget = S.node_count + 8;
-    while (__any_sync(0xFFFFFFFFu, node >= 0)) {
-      if (node >= 0) {
+    // Leaf postponing: a lane that reaches leaf children records them and stops walking;
+    // the warp tests the recorded leaves together once at most kLeafPostponeLanes lanes
+    // can still walk, so the expensive primitive tests run with many lanes at once.  The
+    // prune limits a lane uses while its leaves wait are from its older (farther) best
+    // hit, which only visits more nodes, never fewer: the closest hit is unchanged.
+    int pfirst0 = 0, pmeta0 = 0, pfirst1 = 0, pmeta1 = 0;
+    bool pend = false;
+    while (__any_sync(0xFFFFFFFFu, node >= 0 || pend)) {
+      if (__popc(__ballot_sync(0xFFFFFFFFu, node >= 0 && !pend)) <= kLeafPostponeLanes &&
+          __any_sync(0xFFFFFFFFu, pend)) {
+        int count0 = pend ? (pmeta0 & 0xFFFFFF) : 0, count1 = pend ? (pmeta1 & 0xFFFFFF) : 0;
+        int code0 = pmeta0 >> 24, code1 = pmeta1 >> 24;
+        for (int k = 0; k < count0 + count1; ++k) {
+          bool second = k >= count0;
+          int ref = __ldg(S.refs + (second ? pfirst1 + (k - count0) : pfirst0 + k));
+          int code = second ? code1 : code0;
+          int type = code == 4 ? (int)((unsigned)ref >> kTypeShift) : code;
+          test_ref<METRICS>(S, type, ref & kIndexMask, o, d, dd, b, c);
+        }
+        pend = false;
+        continue;
+      }
+      if (node >= 0 && !pend) {
         const float4* np = S.nodes + 4 * node;
         float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2);
         int4 n3 = __ldg(reinterpret_cast<const int4*>(np + 3));
@@ -541,12 +568,12 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
             if (code1 == 4) c->mixed++; else c->homo++;
           }
         }
-        for (int k = 0; k < count0 + count1; ++k) {
-          bool second = k >= count0;
-          int ref = __ldg(S.refs + (second ? first1 + (k - count0) : first0 + k));
-          int code = second ? code1 : code0;
-          int type = code == 4 ? (int)((unsigned)ref >> kTypeShift) : code;
-          test_ref<METRICS>(S, type, ref & kIndexMask, o, d, dd, b, c);
+        if (count0 + count1 > 0) {
+          pend = true;
+          pfirst0 = first0;
+          pmeta0 = count0 | (code0 << 24);
+          pfirst1 = first1;
+          pmeta1 = count1 | (code1 << 24);
         }
         float plim = prune_limit(b.t);
         int next = (hn && ln >= 0) ? ln : -1;

@@ -106,9 +106,11 @@ rtb_status render_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* ca
 struct FramePlan;
 FramePlan* new_frame_plan();
 void delete_frame_plan(FramePlan* f);
+// tail_per_thread: pixels per resident thread queued one sample per item at the frame's
+// end (0: the default).
 rtb_status plan_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
                       const rtb_render_params* p, float* d_rgb, FramePlan* f, int row0 = 0,
-                      int row_stride = 1);
+                      int row_stride = 1, int tail_per_thread = 0);
 size_t frame_tail_bytes(const FramePlan* f);
 void bind_frame(FramePlan* f, unsigned long long* queue, float* tail, int* abort_flag,
                 unsigned long long* counters);

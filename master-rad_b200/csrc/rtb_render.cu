@@ -359,7 +359,7 @@ void set_tail(FramePlan* f, long long tail_pixels) {
 
 rtb_status plan_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
                       const rtb_render_params* p, float* d_rgb, FramePlan* f, int row0,
-                      int row_stride) {
+                      int row_stride, int tail_per_thread) {
   if (!scene || !cam || !p || !d_rgb) return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "null argument");
   if (p->width < 1 || p->height < 1 || p->samples_per_frame < 1)
     return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "image size and samples must be positive");
@@ -395,7 +395,8 @@ rtb_status plan_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
                   : se < 0 ? 0 : se;
   f->resident = (long long)ctx->sm_count * frame_blocks_per_sm(f->metrics, f->shared_stack) * 128;
   // Tail: about four pixels per resident thread are split into single samples.
-  long long tail_pixels = std::min<long long>(a.pixels, (long long)(RTB_TAIL_FACTOR * f->resident));
+  double per_thread = tail_per_thread > 0 ? (double)tail_per_thread : RTB_TAIL_FACTOR;
+  long long tail_pixels = std::min<long long>(a.pixels, (long long)(per_thread * f->resident));
   set_tail(f, std::min<long long>(tail_pixels, kMaxTailItems / a.spp));
   return RTB_OK;
 }

@@ -31,7 +31,9 @@ class Batch:
         t = None
         if tuning is not None:
             t = N.BatchTuning(int(tuning["threads_per_block"]), int(tuning["job_order"]),
-                              int(tuning.get("branches", 0)))
+                              int(tuning.get("branches", 0)),
+                              int(tuning.get("shared_stack_entries", 0)),
+                              int(tuning.get("tail_pixels_per_thread", 0)))
         h = C.c_void_p()
         ctx.check(ctx.lib.rtb_batch_create(ctx.handle, arr, len(jobs), C.byref(t) if t else None,
                                            C.byref(h)))
@@ -47,7 +49,8 @@ class Batch:
         self.ctx.check(self.ctx.lib.rtb_batch_autotune(self.ctx.handle, self.handle, repeats,
                                                        C.byref(best), C.byref(ms)))
         return {"threads_per_block": best.threads_per_block, "job_order": best.job_order,
-                "branches": best.branches, "ms": ms.value}
+                "branches": best.branches, "shared_stack_entries": best.shared_stack_entries,
+                "tail_pixels_per_thread": best.tail_pixels_per_thread, "ms": ms.value}
 
     def close(self):
         if self.handle:

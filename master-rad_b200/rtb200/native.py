@@ -112,7 +112,8 @@ class CalibrationResult(C.Structure):
 
 
 class BatchTuning(C.Structure):
-    _fields_ = [("threads_per_block", C.c_int), ("job_order", C.c_int), ("branches", C.c_int)]
+    _fields_ = [("threads_per_block", C.c_int), ("job_order", C.c_int), ("branches", C.c_int),
+                ("shared_stack_entries", C.c_int), ("tail_pixels_per_thread", C.c_int)]
 
 
 # Every symbol include/rtb200.h declares, with its ctypes signature.
@@ -159,6 +160,8 @@ SIGNATURES = {
     "rtb_render_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Camera),
                                       C.POINTER(RenderParams), C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p]),
+    "rtb_render_backward_sample": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Camera),
+                                             C.POINTER(RenderParams), FP, FP, FP]),
 }
 
 STATIC_REPLAY_MAX_RAYS = 65536  # RTB_STATIC_REPLAY_MAX_RAYS in include/rtb200.h

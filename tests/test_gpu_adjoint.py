@@ -149,3 +149,26 @@ def test_autograd_function_forward_backward():
     finally:
         ds.close()
         ctx.close()
+
+
+def test_host_buffer_backward_matches_device_backward():
+    """rtb_render_backward_sample (host buffers, the entry a Java Function binds) gives the
+    device entry's gradients (FP32 atomics gather them, so to 1e-5 relative)."""
+    torch = pytest.importorskip("torch")
+    ctx, ds, wl = _setup(torch, n=300, w=32, h=24, spp=4, depth=3)
+    try:
+        import ctypes as C
+        from rtb200 import native as N
+        img = _render(torch, ds, ds.albedo(), ds.emission())
+        adj = (2.0 * img).astype(np.float32)
+        ga, ge = _grads(torch, ds, adj)
+        ha = np.zeros(ds.count * 3, np.float32)
+        he = np.zeros(ds.count * 3, np.float32)
+        ctx.check(ctx.lib.rtb_render_backward_sample(ctx.handle, ds.res.handle, C.byref(ds.cam),
+                                                     C.byref(ds.params), N.fptr(adj),
+                                                     N.fptr(ha), N.fptr(he)))
+        np.testing.assert_allclose(ha.reshape(-1, 3), ga, rtol=1e-5, atol=1e-7)
+        np.testing.assert_allclose(he.reshape(-1, 3), ge, rtol=1e-5, atol=1e-7)
+    finally:
+        ds.close()
+        ctx.close()

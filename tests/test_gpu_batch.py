@@ -87,6 +87,13 @@ def test_batch_tail_spanning_jobs():
             jobs.append((res, w.camera, wdt, hgt, spp, depth, w.frame_index, w.frame_seed, out.data_ptr()))
         tunings = [{"threads_per_block": 128, "job_order": o, "branches": k}
                    for o in (0, 1) for k in (0, 1, 2, 4)]
+        # the autotuner's other knobs: end-of-frame queue granularity and shared-memory
+        # stack depth change the schedule, never the images
+        tunings += [{"threads_per_block": 128, "job_order": 1, "branches": 2,
+                     "shared_stack_entries": se, "tail_pixels_per_thread": tp}
+                    for se, tp in ((-1, 1), (8, 8), (16, 2))]
+        tunings += [{"threads_per_block": 64, "job_order": 0, "branches": 0,
+                     "tail_pixels_per_thread": tp} for tp in (1, 8)]
         for tuning in tunings:
             b = Batch(ctx, jobs, tuning=tuning)
             b.render()
@@ -130,5 +137,25 @@ def test_batch_mixes_tree_and_linear_scenes():
             b.close()
         for _, res in works:
             res.close()
+    finally:
+        ctx.close()
+
+
+def test_batch_rejects_bad_tuning_knobs():
+    torch = pytest.importorskip("torch")
+    ctx = Context(0)
+    try:
+        s = synth.hetero_scene(50, 901, synth.WORKLOAD_IDS["test"], 50)
+        res = ResidentScene.build(ctx, s)
+        out = torch.zeros(8 * 8 * 3, device="cuda")
+        cam = synth.camera_looking_z((0.0, 0.0, -2.9))
+        jobs = [(res, cam, 8, 8, 1, 2, 0, 1, out.data_ptr())]
+        from rtb200 import native as N
+        for bad in ({"shared_stack_entries": 4}, {"tail_pixels_per_thread": 17}):
+            t = {"threads_per_block": 128, "job_order": 0, "branches": 1}
+            t.update(bad)
+            with pytest.raises(ValueError):
+                Batch(ctx, jobs, tuning=t)
+        res.close()
     finally:
         ctx.close()

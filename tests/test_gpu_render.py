@@ -183,3 +183,35 @@ def test_steady_state_samples_and_code_identity():
             t.render_steady_state_sample(rgb, other.scene, w.camera, w.max_depth, 1, 6)
         h = t.compiled_ptx_sha256()
         assert len(h) == 64 and h == t.compiled_ptx_sha256()
+
+
+@pytest.mark.parametrize("entries", [-1, 8, 16])
+def test_shared_stack_entries_knob_keeps_the_image(entries):
+    """rtb_render_params.shared_stack_entries (none, 8 or 16 stack entries per lane in
+    shared memory instead of the by-scene-size default) changes where the traversal stack
+    lives, not the image; other values are refused."""
+    import ctypes as C
+    from rtb200 import native as N
+    from rtb200.tracer import Context, ResidentScene, camera_struct
+    w = _small_hetero(96, 64, 4, 6)
+    ctx = Context(0)
+    try:
+        res = ResidentScene.build(ctx, w.scene)
+        cam = camera_struct(w.camera)
+
+        def frame(se):
+            img = np.zeros(w.width * w.height * 3, np.float32)
+            p = N.RenderParams(w.width, w.height, w.spp, w.max_depth, w.frame_index,
+                               w.frame_seed & 0xFFFFFFFFFFFFFFFF, 1, 0, se)
+            st = ctx.lib.rtb_render_sample(ctx.handle, res.handle, C.byref(cam), C.byref(p),
+                                           N.fptr(img))
+            return st, img
+
+        st0, base = frame(0)
+        st1, img = frame(entries)
+        assert st0 == N.RTB_OK and st1 == N.RTB_OK
+        np.testing.assert_array_equal(img.view(np.int32), base.view(np.int32))
+        assert frame(5)[0] == 1  # RTB_ERR_INVALID_ARGUMENT
+        res.close()
+    finally:
+        ctx.close()
