@@ -57,11 +57,14 @@ FALLBACK_HBM_GBS = 6650.0
 # dram__bytes_read.sum + dram__bytes_write.sum of k_render per sample, from one ncu capture
 # of the same scene at 1024x768x4 spp (profiles/k_render_hetero10k_1024x768x4spp_full.md);
 # workloads without a capture report null traffic.
-TRAFFIC_BYTES_PER_SAMPLE = {"hetero": (22.41e6 + 115.70e6) / 3145728}
-# smsp__inst_executed.sum of k_render per sample from the same capture (9.28 G warp
+TRAFFIC_BYTES_PER_SAMPLE = {"hetero": (18.30e6 + 110.59e6) / 3145728}
+# smsp__inst_executed.sum of k_render per sample from the same capture (9.136 G warp
 # instructions for 3,145,728 samples), for the issue bound: warp instructions per second
 # against one instruction per cycle on each of the 4 schedulers of every SM.
-INST_PER_SAMPLE = {"hetero": 9.28e9 / 3145728}
+INST_PER_SAMPLE = {"hetero": 9.136e9 / 3145728}
+# smsp__thread_inst_executed_per_inst_executed of the same capture: active lanes per warp
+# instruction, which scales the issue bound to lane-instructions doing useful work.
+LANES_PER_INST = {"hetero": 9.13}
 
 
 def issue_roofline(workload, samples, launch_ms, sm_count, sm_mhz):
@@ -71,11 +74,14 @@ def issue_roofline(workload, samples, launch_ms, sm_count, sm_mhz):
     inst = INST_PER_SAMPLE[workload] * samples
     achieved = inst / (launch_ms / 1e3)
     peak = sm_count * 4 * sm_mhz * 1e6
+    lanes = LANES_PER_INST[workload]
     return {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "warp-inst/s",
             "frac": achieved / peak, "inst_per_launch": inst,
+            "active_lanes_per_inst": lanes, "useful_lane_frac": achieved / peak * lanes / 32.0,
             "note": "instructions per sample from the ncu capture of a 1024x768x4spp frame of "
                     "the same scene, scaled by samples; peak = SMs x 4 schedulers x the SM "
-                    "clock sampled during the timed frames"}
+                    "clock sampled during the timed frames; useful_lane_frac also counts the "
+                    "lanes a warp instruction leaves idle (divergent paths)"}
 
 
 def parse_args(argv=None):
@@ -88,6 +94,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ref-kernel", action="store_true")
+    ap.add_argument("--no-other-configs", action="store_true",
+                    help="skip the other configurations measured after the headline line's timing")
     ap.add_argument("--split", default="rows", choices=["rows", "frames"],
                     help="with N > 1 GPUs: rows -- every step is one frame whose rows are dealt "
                          "out across the ranks and all-gathered (strong scaling); frames -- "
@@ -342,27 +350,18 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_batched(args, rank=0, world=1, local=0):
-    """The 64-scene batch (primitive counts log-uniform in [1k, 200k], resolutions from
-    {256^2, 512^2, 1024^2}, 16 or 64 spp, depth 6): per-scene frames launched back to back
-    versus the batch replayed from its CUDA graph after autotuning (one shared-queue kernel
-    over all jobs, or the jobs' own frames spread over concurrent graph branches).  With
-    several ranks the scenes are dealt round-robin, each rank batching its own on its GPU;
-    the rate is all 64 scenes' samples over the slowest rank's time."""
+def batched_measure(ctx, local, works, steps, warmup, world=1, autotune=True):
+    """Per-scene frames launched back to back versus the batch replayed from its CUDA graph
+    (after autotuning, or with the default tuning): CUDA-event milliseconds of each, the
+    tuning, whether every image is identical, and the device build time of the scenes."""
     import torch
     from rtb200.batch import Batch
-    init_ranks(world, local)
-    ctx = Context(local)
     lib = ctx.lib
-    all_works = synth.batched_workloads()
-    total_samples = sum(w.width * w.height * w.spp for w in all_works)
-    works = [all_works[i] for i in scenes_of_rank(len(all_works), rank, world)]
     t0 = time.perf_counter()
     scenes = [ResidentScene.build(ctx, w.scene) for w in works]
     build_ms = sum(r.stats.build_ms for r in scenes)
     build_wall = time.perf_counter() - t0
     outs = [torch.zeros(w.width * w.height * 3, dtype=torch.float32, device="cuda") for w in works]
-    samples = sum(w.width * w.height * w.spp for w in works)
     stream = torch.cuda.Stream(device=local)
     sh = C.c_void_p(stream.cuda_stream)
 
@@ -377,21 +376,21 @@ def run_batched(args, rank=0, world=1, local=0):
     jobs = [(r, w.camera, w.width, w.height, w.spp, w.max_depth, w.frame_index, w.frame_seed,
              o.data_ptr()) for w, r, o in zip(works, scenes, outs)]
     batch = Batch(ctx, jobs)
-    tuned = batch.autotune(repeats=1)
+    tuned = batch.autotune(repeats=1) if autotune else None
 
     def timed(fn):
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             fn()
         stream.synchronize()
         barrier(world)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             fn()
         e1.record(stream)
         e1.synchronize()
         barrier(world)
-        return e0.elapsed_time(e1) / args.steps
+        return e0.elapsed_time(e1) / steps
 
     seq_ms = max_over_ranks(timed(sequential))
     ref_imgs = [o.cpu().numpy().copy() for o in outs]
@@ -399,8 +398,30 @@ def run_batched(args, rank=0, world=1, local=0):
     same = all(np.array_equal(o.cpu().numpy().view(np.int32), r.view(np.int32))
                for o, r in zip(outs, ref_imgs))
     differ = max_over_ranks(0.0 if same else 1.0)
+    branches = tuned["branches"] if tuned else 4
     # each frame or shared-queue launch is followed by its single-sample tail sum
-    launches = max_over_ranks(args.steps * 2 * (len(works) if tuned["branches"] > 0 else 1))
+    launches = max_over_ranks(steps * 2 * (len(works) if branches > 0 else 1))
+    batch.close()
+    for r in scenes:
+        r.close()
+    return {"seq_ms": seq_ms, "bat_ms": bat_ms, "tuning": tuned, "identical": differ == 0.0,
+            "build_ms": build_ms, "build_wall_s": build_wall, "launches": int(launches)}
+
+
+def run_batched(args, rank=0, world=1, local=0):
+    """The 64-scene batch (primitive counts log-uniform in [1k, 200k], resolutions from
+    {256^2, 512^2, 1024^2}, 16 or 64 spp, depth 6): per-scene frames launched back to back
+    versus the batch replayed from its CUDA graph after autotuning (one shared-queue kernel
+    over all jobs, or the jobs' own frames spread over concurrent graph branches).  With
+    several ranks the scenes are dealt round-robin, each rank batching its own on its GPU;
+    the rate is all 64 scenes' samples over the slowest rank's time."""
+    init_ranks(world, local)
+    ctx = Context(local)
+    all_works = synth.batched_workloads()
+    total_samples = sum(w.width * w.height * w.spp for w in all_works)
+    works = [all_works[i] for i in scenes_of_rank(len(all_works), rank, world)]
+    m = batched_measure(ctx, local, works, args.steps, args.warmup, world)
+    seq_ms, bat_ms = m["seq_ms"], m["bat_ms"]
     line = {"metric": "Msamples/s", "value": total_samples / (bat_ms / 1e3) / 1e6,
             "unit": "Msamples/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": bat_ms, "higher_is_better": True, "scaling": "strong",
@@ -411,16 +432,84 @@ def run_batched(args, rank=0, world=1, local=0):
                        "parallelism": ("scenes round-robin over ranks" if world > 1
                                        else "single GPU")},
             "sequential": {"value": total_samples / (seq_ms / 1e3) / 1e6, "ms_per_step": seq_ms},
-            "batched_over_sequential": seq_ms / bat_ms, "tuning": tuned,
-            "images_identical": differ == 0.0, "device_build_ms_total": build_ms,
-            "build_wall_s": build_wall, "gpu_launches": int(launches) * world}
+            "batched_over_sequential": seq_ms / bat_ms, "tuning": m["tuning"],
+            "images_identical": m["identical"], "device_build_ms_total": m["build_ms"],
+            "build_wall_s": m["build_wall_s"], "gpu_launches": m["launches"] * world}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    batch.close()
-    for r in scenes:
-        r.close()
     ctx.close()
     finish_ranks(world)
+
+
+def frames_measure(ctx, w, steps, warmup, flush, stream, ref_frames=0):
+    """Device build and frames of one configuration on one GPU: median build ms, Msamples/s
+    over `steps` frames (CUDA events around each frame, L2 flushed before each outside the
+    events), and optionally the reference kernel on the same frame (ref_kernel_leg)."""
+    import torch
+    builds = []
+    for i in range(2):
+        r = ResidentScene.build(ctx, w.scene)
+        builds.append(r.stats.build_ms)
+        if i == 0:
+            r.close()
+    res = r
+    out = torch.empty(w.width * w.height * 3, dtype=torch.float32, device="cuda")
+    cam = camera_struct(w.camera)
+    sh = C.c_void_p(stream.cuda_stream)
+    ms = []
+    for i in range(warmup + steps):
+        p = N.RenderParams(w.width, w.height, w.spp, w.max_depth, 2000 + i,
+                           w.frame_seed & 0xFFFFFFFFFFFFFFFF, 1, 0, 0)
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.check(ctx.lib.rtb_render_device(ctx.handle, res.handle, C.byref(cam), C.byref(p),
+                                                C.c_void_p(out.data_ptr()), sh))
+            e1.record(stream)
+        e1.synchronize()
+        if i >= warmup:
+            ms.append(e0.elapsed_time(e1))
+    samples = w.width * w.height * w.spp
+    d = {"value": samples / (statistics.mean(ms) / 1e3) / 1e6, "unit": "Msamples/s",
+         "ms_per_frame": statistics.mean(ms), "frames": steps, "build_ms": builds[-1],
+         "primitives": w.scene.bounded_primitive_count(),
+         "frame": "%dx%d %dspp depth%d" % (w.width, w.height, w.spp, w.max_depth)}
+    if ref_frames:
+        rk = ref_kernel_leg(w, _Tree(res.download_bvh()), ref_frames, flush.numel() * 4)
+        if rk is not None:
+            d["ref_kernel"] = {"value": rk["value"], "ms_per_frame": rk["fmad"]["ms_per_frame"],
+                               "variant": "fmad"}
+            d["vs_ref_kernel"] = d["value"] / rk["value"]
+    res.close()
+    return d
+
+
+def other_configs(ctx, local, flush):
+    """The benchmark's other configurations, measured once after the headline timing so that
+    one default run shows them all: the plain 64-sphere frame (with the reference kernel
+    beside it), the 1M-primitive scene (device build and frames), the 64-scene batch with
+    the default tuning (versus its scenes' frames back to back) and the differentiable
+    configuration (forward, backward and the finite-difference check)."""
+    import torch
+    stream = torch.cuda.Stream(device=local)
+    out = {}
+    out["C1_plain"] = frames_measure(ctx, synth.plain_workload(), 10, 3, flush, stream, ref_frames=3)
+    out["C3_scale"] = frames_measure(ctx, synth.scale_workload(), 2, 1, flush, stream)
+    works = synth.batched_workloads()
+    m = batched_measure(ctx, local, works, 1, 1, autotune=False)
+    samples = sum(w.width * w.height * w.spp for w in works)
+    out["C4_batched"] = {"value": samples / (m["bat_ms"] / 1e3) / 1e6, "unit": "Msamples/s",
+                         "ms_per_batch": m["bat_ms"], "tuning": "default (per-job frames, 4 branches)",
+                         "sequential_value": samples / (m["seq_ms"] / 1e3) / 1e6,
+                         "batched_over_sequential": m["seq_ms"] / m["bat_ms"],
+                         "images_identical": m["identical"], "scenes": len(works)}
+    a = adjoint_measure(ctx, local, 3, 1)
+    out["C5_adjoint"] = {"forward_ms": a["forward_ms"], "backward_ms": a["backward_ms"],
+                         "backward_over_forward": a["backward_ms"] / a["forward_ms"],
+                         "backward_value": a["samples"] / (a["backward_ms"] / 1e3) / 1e6,
+                         "unit": "Msamples/s", "fd_check": a["fd_check"]}
+    return out
 
 
 FD_SMALL = 1e-2  # |FD| below this fraction of its group's typical gradient counts as small
@@ -478,18 +567,15 @@ def fd_check(g, n_albedo, loss, alb0, emi0, count, rng, h=1e-3):
             "rows": rows}
 
 
-def run_adjoint(args, rank=0, world=1, local=0):
-    """The differentiable workload: 4096-primitive mixed scene, 512x512, 32 spp, depth 6; L2
-    image loss against a target rendered with albedos perturbed by N(0, 0.05) (12-uniform
-    approximation, clamped to [0, 1]); forward frame vs path-replay backward time, and the
-    error against central finite differences (h = 1e-3, common random numbers, FP64 loss) on
-    64 parameters drawn uniformly from all albedo and emission components (fd_check).  One
-    backward pass does not shard: with several ranks each runs an independent replica on its
-    GPU, and the rate is all replicas' samples over the slowest rank's backward time."""
+def adjoint_measure(ctx, local, steps, warmup, world=1, fd_count=64):
+    """The differentiable configuration: 4096-primitive mixed scene, 512x512, 32 spp, depth
+    6; L2 image loss against a target rendered with albedos perturbed by N(0, 0.05)
+    (12-uniform approximation, clamped to [0, 1]); forward frame vs path-replay backward
+    time (CUDA events), and the error against central finite differences (h = 1e-3, common
+    random numbers, FP64 loss) on ``fd_count`` parameters drawn uniformly from all albedo and
+    emission components (fd_check)."""
     import torch
     from rtb200.diff import DifferentiableScene
-    init_ranks(world, local)
-    ctx = Context(local)
     w = synth.adjoint_workload()
     ds = DifferentiableScene(ctx, w.scene, w.width, w.height, w.spp, w.max_depth, w.camera,
                              w.frame_index, w.frame_seed)
@@ -520,40 +606,51 @@ def run_adjoint(args, rank=0, world=1, local=0):
     fwd, bwd = [], []
     torch.cuda.synchronize()
     barrier(world)
-    for i in range(args.warmup + args.steps):
+    for i in range(warmup + steps):
         e0.record(sobj)
         ds.render_into(img.data_ptr(), stream)
         e1.record(sobj)
         e1.synchronize()
-        if i >= args.warmup:
+        if i >= warmup:
             fwd.append(e0.elapsed_time(e1))
         e0.record(sobj)
         ds.backward_into(adj.data_ptr(), ga.data_ptr(), ge.data_ptr(), stream)
         e1.record(sobj)
         e1.synchronize()
-        if i >= args.warmup:
+        if i >= warmup:
             bwd.append(e0.elapsed_time(e1))
     sobj.synchronize()
     g = np.concatenate([ga.cpu().numpy(), ge.cpu().numpy()]).astype(np.float64)
     fd = fd_check(g, ga.numel(), lambda a, e: float(np.sum((render(a, e) - target) ** 2)),
-                  alb0, emi0, 64, np.random.default_rng(1))
+                  alb0, emi0, fd_count, np.random.default_rng(1))
     fd.pop("rows")
-    samples = w.width * w.height * w.spp
-    f_ms = max_over_ranks(statistics.mean(fwd))
-    b_ms = max_over_ranks(statistics.mean(bwd))
-    line = {"metric": "Msamples/s", "value": world * samples / (b_ms / 1e3) / 1e6,
+    out = {"samples": w.width * w.height * w.spp, "materials": ds.count,
+           "forward_ms": max_over_ranks(statistics.mean(fwd)),
+           "backward_ms": max_over_ranks(statistics.mean(bwd)), "fd_check": fd}
+    ds.close()
+    return out
+
+
+def run_adjoint(args, rank=0, world=1, local=0):
+    """The differentiable workload (adjoint_measure).  One backward pass does not shard: with
+    several ranks each runs an independent replica on its GPU, and the rate is all replicas'
+    samples over the slowest rank's backward time."""
+    init_ranks(world, local)
+    ctx = Context(local)
+    m = adjoint_measure(ctx, local, args.steps, args.warmup, world)
+    f_ms, b_ms = m["forward_ms"], m["backward_ms"]
+    line = {"metric": "Msamples/s", "value": world * m["samples"] / (b_ms / 1e3) / 1e6,
             "unit": "Msamples/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": b_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "adjoint-4k 512x512 32spp depth6", "materials": ds.count,
-                       "parameters": 6 * ds.count,
+            "config": {"workload": "adjoint-4k 512x512 32spp depth6", "materials": m["materials"],
+                       "parameters": 6 * m["materials"],
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "forward_ms": f_ms, "backward_ms": b_ms, "backward_over_forward": b_ms / f_ms,
-            "fd_check": fd,
+            "fd_check": m["fd_check"],
             "gpu_launches": world * args.steps}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    ds.close()
     ctx.close()
     finish_ranks(world)
 
@@ -804,6 +901,8 @@ def main():
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        if world == 1 and args.workload == "hetero" and not args.no_other_configs:
+            line["other_configs"] = other_configs(ctx, local, flush)
         if world == 1 and not args.no_ref_kernel:
             frames = args.ref_frames or (1 if args.workload == "scale" else 3)
             rk = ref_kernel_leg(w, _Tree(res.download_bvh()), frames, flush.numel() * 4)

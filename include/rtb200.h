@@ -74,8 +74,10 @@ typedef struct {
 } rtb_bvh_desc;
 
 /* BvhBuildConfig (gfxlab/gpu/BvhBuildConfig.java:6-15); mode is a BvhBuildMode ordinal
- * (0 UNIFORM_SAH, 1 WEIGHTED_SAH, 2 PER_TYPE_SAH, 3 PER_TYPE_WEIGHTED_SAH, 6 SAH_ROTATIONS,
- * 7 WEIGHTED_SAH_ROTATIONS; the SBVH modes 4 and 5 return RTB_ERR_UNSUPPORTED). */
+ * (0 UNIFORM_SAH, 1 WEIGHTED_SAH, 2 PER_TYPE_SAH, 3 PER_TYPE_WEIGHTED_SAH, 4 UNIFORM_SBVH,
+ * 5 WEIGHTED_SBVH, 6 SAH_ROTATIONS, 7 WEIGHTED_SAH_ROTATIONS).  The SBVH modes build on the
+ * host in depth-first order (their global reference budget makes every split depend on the
+ * ones before it); the others build on the device.  The binned builder takes modes 0-3. */
 typedef struct {
   int mode;
   int leaf_size;
@@ -85,8 +87,7 @@ typedef struct {
 } rtb_build_config;
 
 /* BvhBuildOptions (gfxlab/gpu/BvhBuildOptions.java:4-33); defaults 128, 2.0, 8, 16, 1e-5, 4.
- * The device builders read rotation_passes (rotation modes); the spatial-split fields
- * belong to the SBVH modes. */
+ * rotation_passes belongs to the rotation modes, the other fields to the SBVH modes. */
 typedef struct {
   int spatial_bins;
   double max_reference_multiplier;
@@ -102,9 +103,13 @@ typedef struct {
   int min_leaf_occupancy, max_leaf_occupancy;
   double generalized_sah_cost, uniform_sah_cost, weighted_sah_cost;
   long long bytes;
-  double build_ms;          /* CUDA-event time of the device build */
-  int sequential_nodes;     /* nodes whose split needed the exact sequential weight order */
+  double build_ms;          /* build time: CUDA events for the device builders, host wall
+                               time for the SBVH modes */
+  int sequential_nodes;     /* nodes above 256 primitives whose split the count-based
+                               weights could not certify, summed in the sequential order */
   int rotation_count;       /* BvhStats.rotationCount of the rotation modes */
+  int spatial_split_count;  /* BvhStats.spatialSplitCount of the SBVH modes */
+  int duplicate_reference_count; /* BvhStats.duplicateReferenceCount (references - primitives) */
 } rtb_bvh_stats;
 
 /* GpuCamera (gfxlab/gpu/GpuCamera.java): direction = forward + right u + up v. */

@@ -12,7 +12,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "rtb200", "librtb200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-SOURCES = ["rtb_abi.cu", "rtb_scene.cu", "rtb_render.cu", "rtb_build.cu", "rtb_binned.cu", "rtb_static.cu", "rtb_batch.cu", "rtb_adjoint.cu", "rtb_calibrate.cu"]
+SOURCES = ["rtb_abi.cu", "rtb_scene.cu", "rtb_render.cu", "rtb_build.cu", "rtb_binned.cu", "rtb_static.cu", "rtb_batch.cu", "rtb_adjoint.cu", "rtb_calibrate.cu",
+           "rtb_sbvh.cu"]
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-fmad=false",
          "-std=c++17", "-shared", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "-DRTB_BUILD"]

@@ -27,6 +27,9 @@
 //    node's current order)) uses the parent's split-axis order, which is the order the
 //    Java primitives array holds when build() reaches the node.
 // The file is compiled with -fmad=false: no double expression is contracted.
+#include <thrust/iterator/counting_iterator.h>
+#include <thrust/iterator/transform_iterator.h>
+
 #include "rtb_build_common.cuh"
 
 namespace rtb {
@@ -45,20 +48,23 @@ __global__ void k_type_keys(const Prims P, const int* idx, int n, int* keys) {
 }
 
 
-__global__ void k_gather_boxes(const Prims P, const int* idx, int n, bool reverse, const int* key,
-                               Box* out, int* out_key) {
+// The primitives' boxes in one axis order (the suffix scan reads the same array backwards).
+__global__ void k_gather_boxes(const Prims P, const int* idx, int n, Box* out) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  int src = reverse ? n - 1 - j : j;
-  int p = idx[src];
-  Box b;
-  for (int k = 0; k < 3; ++k) {
-    b.mn[k] = P.lo[k][p];
-    b.mx[k] = P.hi[k][p];
-  }
-  out[j] = b;
-  out_key[j] = key[src];
+  if (j < n) out[j] = P.box[idx[j]];
 }
+
+// Position j of the reversed order: element n - 1 - j (input iterators for the suffix scans).
+struct ReverseBox {
+  const Box* a;
+  int n;
+  __host__ __device__ __forceinline__ Box operator()(int j) const { return a[n - 1 - j]; }
+};
+struct ReverseKey {
+  const int* a;
+  int n;
+  __host__ __device__ __forceinline__ int operator()(int j) const { return a[n - 1 - j]; }
+};
 
 __global__ void k_gather_weights(const Prims P, const int* idx, int n, double* wpos) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -392,14 +398,17 @@ __global__ void k_argmin_flat(int blocks_total, const double* part_cost, const l
 // the per-level passes over all primitives (scans, gathers, argmin blocks) that dominate
 // the deep levels.
 constexpr int kSubtreeSize = kSeqNodeSize;
-constexpr int kSubtreeWarps = 2;
+constexpr int kSubtreeThreads = 96;  // one warp per axis
 
 struct SubtreeSmem {
-  int idx[3][kSubtreeSize];
-  Box sbox[kSubtreeSize];
-  double sw[kSubtreeSize];
-  int tmp[kSubtreeSize];
-  int stack[kSubtreeSize];
+  int idx[3][kSubtreeSize];     // the subtree's three axis orders
+  Box sbox[3][kSubtreeSize];    // per axis: suffix boxes of the current node
+  double sw[3][kSubtreeSize];   // per axis: suffix weights
+  int tmp[3][kSubtreeSize];     // per axis: partition scratch
+  int stack[kSubtreeSize];      // pending nodes (depth first)
+  double best_cost[3];
+  long long best_flat[3];
+  int sp, child;
 };
 
 __device__ __forceinline__ Box empty_box() {
@@ -411,14 +420,7 @@ __device__ __forceinline__ Box empty_box() {
   return b;
 }
 
-__device__ __forceinline__ Box prim_box(const Prims& P, int p) {
-  Box b;
-  for (int k = 0; k < 3; ++k) {
-    b.mn[k] = P.lo[k][p];
-    b.mx[k] = P.hi[k][p];
-  }
-  return b;
-}
+__device__ __forceinline__ Box prim_box(const Prims& P, int p) { return P.box[p]; }
 
 // Inclusive union over lanes 0..lane (min / max are exact in any order).
 __device__ __forceinline__ Box warp_union_scan(Box b, int lane) {
@@ -454,28 +456,36 @@ __device__ __forceinline__ double warp_sequential_sum(double w, double& acc, int
   return mine;
 }
 
-__global__ void __launch_bounds__(32 * kSubtreeWarps) k_subtrees(
+__device__ __forceinline__ bool lex_less(double c, long long f, double bc, long long bf) {
+  return c < bc || (c == bc && f < bf);
+}
+
+// One block of three warps per subtree root: warp a sweeps axis a of the current node,
+// the block takes the first minimum over the three axes' winners, and the warps of the two
+// other axes partition their orders.  Every decision is computed identically by all threads
+// (or broadcast through shared memory), so the block's barriers are uniform.
+__global__ void __launch_bounds__(kSubtreeThreads) k_subtrees(
     const Prims P, IdxSet I, Nodes N, const int* roots, const int* root_count, int leaf_size,
     double traversal, int* node_counter, int* stats, unsigned char* side) {
-  __shared__ SubtreeSmem smem[kSubtreeWarps];
+  __shared__ SubtreeSmem sm;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = blockIdx.x * kSubtreeWarps + warp;
-  if (g >= *root_count) return;
-  SubtreeSmem& sm = smem[warp];
-  const int root = roots[g];
+  if ((int)blockIdx.x >= *root_count) return;
+  const int root = roots[blockIdx.x];
   const int rs = N.start[root], re = N.end[root], M = re - rs;
   for (int a = 0; a < 3; ++a)
-    for (int i = lane; i < M; i += 32) sm.idx[a][i] = I.a[a][rs + i];
-  int sp = 0;
-  if (lane == 0) sm.stack[0] = root;
-  sp = 1;
-  __syncwarp();
-  while (sp > 0) {
-    const int node = sm.stack[--sp];
-    __syncwarp();
+    for (int i = threadIdx.x; i < M; i += kSubtreeThreads) sm.idx[a][i] = I.a[a][rs + i];
+  if (threadIdx.x == 0) {
+    sm.stack[0] = root;
+    sm.sp = 1;
+  }
+  __syncthreads();
+  while (sm.sp > 0) {
+    const int node = sm.stack[sm.sp - 1];
+    __syncthreads();
+    if (threadIdx.x == 0) sm.sp--;
     const int s = N.start[node], e = N.end[node], m = e - s, lo = s - rs;
     const int oa = N.order_axis[node];
-    // node bounds
+    // node bounds (every warp computes the same union)
     Box nb = empty_box();
     for (int i = lane; i < m; i += 32) nb = BoxUnion()(nb, prim_box(P, sm.idx[0][lo + i]));
     for (int off = 16; off > 0; off >>= 1) {
@@ -487,64 +497,73 @@ __global__ void __launch_bounds__(32 * kSubtreeWarps) k_subtrees(
       nb = BoxUnion()(nb, o);
     }
     const double node_a = surface_area(nb) * traversal;
+    // this warp's axis
     double best = CUDART_INF;
     long long best_flat = 0x7FFFFFFFFFFFFFFFLL;
-    if (m > 1) {
-      for (int a = 0; a < 3; ++a) {
-        const int* ix = sm.idx[a] + lo;
-        double ext = P.cen[a][ix[m - 1]] - P.cen[a][ix[0]];
-        if (!(ext > 1.0e-12)) continue;
-        // suffix boxes and weights, from the last position down (GpuScene.java:1476-1480)
-        Box carry = empty_box();
-        double acc = 0.0;
-        for (int base = 0; base < m; base += 32) {
-          int q = m - 1 - (base + lane);
-          int valid = min(32, m - base);
-          Box b = q >= 0 ? prim_box(P, ix[q]) : empty_box();
-          double w = q >= 0 ? P.w[ix[q]] : 0.0;
-          b = BoxUnion()(warp_union_scan(b, lane), carry);
-          double sw = warp_sequential_sum(w, acc, lane, valid);
-          if (q >= 0) {
-            sm.sbox[lo + q] = b;
-            sm.sw[lo + q] = sw;
-          }
-          carry = warp_bcast(b, 31);
+    const int a = warp;
+    const int* ix = sm.idx[a] + lo;
+    if (m > 1 && P.cen[a][ix[m - 1]] - P.cen[a][ix[0]] > 1.0e-12) {
+      // suffix boxes and weights, from the last position down (GpuScene.java:1476-1480)
+      Box carry = empty_box();
+      double acc = 0.0;
+      for (int base = 0; base < m; base += 32) {
+        int q = m - 1 - (base + lane);
+        int valid = min(32, m - base);
+        Box b = q >= 0 ? prim_box(P, ix[q]) : empty_box();
+        double w = q >= 0 ? P.w[ix[q]] : 0.0;
+        b = BoxUnion()(warp_union_scan(b, lane), carry);
+        double sw = warp_sequential_sum(w, acc, lane, valid);
+        if (q >= 0) {
+          sm.sbox[a][lo + q] = b;
+          sm.sw[a][lo + q] = sw;
         }
-        __syncwarp();
-        // prefix pass and the cost of putting local positions [0, i) left (1470-1475, 1482-1485)
-        carry = empty_box();
-        acc = 0.0;
-        for (int base = 0; base < m; base += 32) {
-          int li = base + lane;
-          int valid = min(32, m - base);
-          Box b = li < m ? prim_box(P, ix[li]) : empty_box();
-          double w = li < m ? P.w[ix[li]] : 0.0;
-          b = BoxUnion()(warp_union_scan(b, lane), carry);
-          double pw = warp_sequential_sum(w, acc, lane, valid);
-          int i = li + 1;  // split after li
-          if (i < m) {
-            double bl = surface_area(b) * pw;
-            double d = surface_area(sm.sbox[lo + i]) * sm.sw[lo + i];
-            double c = (node_a + bl) + d;
-            long long flat = (long long)a * m + i;
-            if (c < best || (c == best && flat < best_flat)) {
-              best = c;
-              best_flat = flat;
-            }
+        carry = warp_bcast(b, 31);
+      }
+      __syncwarp();
+      // prefix pass and the cost of putting local positions [0, i) left (1470-1475, 1482-1485)
+      carry = empty_box();
+      acc = 0.0;
+      for (int base = 0; base < m; base += 32) {
+        int li = base + lane;
+        int valid = min(32, m - base);
+        Box b = li < m ? prim_box(P, ix[li]) : empty_box();
+        double w = li < m ? P.w[ix[li]] : 0.0;
+        b = BoxUnion()(warp_union_scan(b, lane), carry);
+        double pw = warp_sequential_sum(w, acc, lane, valid);
+        int i = li + 1;  // split after li
+        if (i < m) {
+          double bl = surface_area(b) * pw;
+          double d = surface_area(sm.sbox[a][lo + i]) * sm.sw[a][lo + i];
+          double c = (node_a + bl) + d;
+          long long flat = (long long)a * m + i;
+          if (lex_less(c, flat, best, best_flat)) {
+            best = c;
+            best_flat = flat;
           }
-          carry = warp_bcast(b, 31);
         }
-        __syncwarp();
+        carry = warp_bcast(b, 31);
+      }
+      for (int off = 16; off > 0; off >>= 1) {
+        double oc = __shfl_xor_sync(0xFFFFFFFFu, best, off);
+        long long of = __shfl_xor_sync(0xFFFFFFFFu, best_flat, off);
+        if (lex_less(oc, of, best, best_flat)) {
+          best = oc;
+          best_flat = of;
+        }
       }
     }
-    for (int off = 16; off > 0; off >>= 1) {
-      double oc = __shfl_xor_sync(0xFFFFFFFFu, best, off);
-      long long of = __shfl_xor_sync(0xFFFFFFFFu, best_flat, off);
-      if (oc < best || (oc == best && of < best_flat)) {
-        best = oc;
-        best_flat = of;
-      }
+    if (lane == 0) {
+      sm.best_cost[a] = best;
+      sm.best_flat[a] = best_flat;
     }
+    __syncthreads();
+    best = sm.best_cost[0];
+    best_flat = sm.best_flat[0];
+    for (int k = 1; k < 3; ++k)
+      if (lex_less(sm.best_cost[k], sm.best_flat[k], best, best_flat)) {
+        best = sm.best_cost[k];
+        best_flat = sm.best_flat[k];
+      }
     // leaf rule (GpuScene.java:1435-1441), the weight sum in the node's current order
     bool leaf = m == 1 || best == CUDART_INF;
     if (!leaf && m <= leaf_size) {
@@ -552,26 +571,24 @@ __global__ void __launch_bounds__(32 * kSubtreeWarps) k_subtrees(
       for (int j = 0; j < m; ++j) wsum = wsum + P.w[oa < 0 ? s + j : sm.idx[oa][lo + j]];
       if (!(best < surface_area(nb) * wsum)) leaf = true;
     }
-    if (lane == 0) {
+    if (threadIdx.x == 0) {
       N.bounds[node] = nb;
       N.split_axis[node] = -1;
     }
     if (leaf) {
-      if (lane == 0) {
+      if (threadIdx.x == 0) {
         N.leaf[node] = 1;
         atomicAdd(stats + 0, 1);
         atomicMin(stats + 1, m);
         atomicMax(stats + 2, m);
         atomicMax(stats + 3, N.depth[node]);
       }
-      __syncwarp();
+      __syncthreads();
       continue;
     }
     const int axis = (int)(best_flat / m), pos = (int)(best_flat % m);
-    int l = 0;
-    if (lane == 0) {
-      l = atomicAdd(node_counter, 2);
-      int r = l + 1;
+    if (threadIdx.x == 0) {
+      int l = atomicAdd(node_counter, 2), r = l + 1;
       N.leaf[node] = 0;
       N.left[node] = l;
       N.right[node] = r;
@@ -585,13 +602,16 @@ __global__ void __launch_bounds__(32 * kSubtreeWarps) k_subtrees(
       N.depth[l] = N.depth[r] = N.depth[node] + 1;
       N.leaf[l] = N.leaf[r] = 0;
       atomicMax(stats + 3, N.depth[node] + 1);
+      sm.stack[sm.sp] = r;
+      sm.stack[sm.sp + 1] = l;
+      sm.sp += 2;
     }
-    l = __shfl_sync(0xFFFFFFFFu, l, 0);
     // stable partition of the other two axis orders by side
-    for (int i = lane; i < m; i += 32) side[sm.idx[axis][lo + i]] = i >= pos ? 1 : 0;
-    __syncwarp();
-    for (int a = 0; a < 3; ++a) {
-      if (a == axis) continue;
+    if (warp == axis)
+      for (int i = lane; i < m; i += 32) side[sm.idx[axis][lo + i]] = i >= pos ? 1 : 0;
+    __syncthreads();
+    if (warp != axis) {
+      int* t = sm.tmp[a];
       int nl = 0;
       for (int base = 0; base < m; base += 32) {
         int li = base + lane;
@@ -599,7 +619,7 @@ __global__ void __launch_bounds__(32 * kSubtreeWarps) k_subtrees(
         int p = in ? sm.idx[a][lo + li] : 0;
         bool left = in && side[p] == 0;
         unsigned bal = __ballot_sync(0xFFFFFFFFu, left);
-        if (left) sm.tmp[lo + nl + __popc(bal & ((1u << lane) - 1u))] = p;
+        if (left) t[nl + __popc(bal & ((1u << lane) - 1u))] = p;
         nl += __popc(bal);
       }
       int nr = 0;
@@ -609,22 +629,16 @@ __global__ void __launch_bounds__(32 * kSubtreeWarps) k_subtrees(
         int p = in ? sm.idx[a][lo + li] : 0;
         bool right = in && side[p] != 0;
         unsigned bal = __ballot_sync(0xFFFFFFFFu, right);
-        if (right) sm.tmp[lo + pos + nr + __popc(bal & ((1u << lane) - 1u))] = p;
+        if (right) t[pos + nr + __popc(bal & ((1u << lane) - 1u))] = p;
         nr += __popc(bal);
       }
       __syncwarp();
-      for (int i = lane; i < m; i += 32) sm.idx[a][lo + i] = sm.tmp[lo + i];
-      __syncwarp();
+      for (int i = lane; i < m; i += 32) sm.idx[a][lo + i] = t[i];
     }
-    if (lane == 0) {
-      sm.stack[sp] = l + 1;
-      sm.stack[sp + 1] = l;
-    }
-    sp += 2;
-    __syncwarp();
+    __syncthreads();
   }
   for (int a = 0; a < 3; ++a)
-    for (int i = lane; i < M; i += 32) I.a[a][rs + i] = sm.idx[a][i];
+    for (int i = threadIdx.x; i < M; i += kSubtreeThreads) I.a[a][rs + i] = sm.idx[a][i];
 }
 
 // Nodes per depth, then all nodes listed level by level (the finishing passes walk them).
@@ -868,6 +882,7 @@ rtb_status build_bvh(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_bui
 rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_build_config* cfg,
                              const rtb_build_options* options, rtb_scene** out, rtb_bvh_stats* stats) {
   if (!out) return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "null argument");
+  if (cfg && (cfg->mode == 4 || cfg->mode == 5)) return build_bvh_sbvh(ctx, desc, cfg, options, out, stats);
   BuildCfg c;
   bool per_type = false;
   rtb_status st = build_setup(ctx, desc, cfg, c, per_type, true);
@@ -897,7 +912,6 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
   Nodes N = alloc_nodes(W, cap);
   int* level_of = W.alloc<int>(cap);
   int* key = W.alloc<int>(n);
-  int* key_rev = W.alloc<int>(n);
   Box* boxes = W.alloc<Box>(n);
   Box* pre_ax[3];
   Box* suf_ax[3];
@@ -954,6 +968,14 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
   size_t tmp_bytes = 0, b1 = 0, b2 = 0, b3 = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, b1, skeys, skeys2, svals, svals, n);
   cub::DeviceScan::InclusiveScanByKey(nullptr, b2, key, boxes, pre0, BoxUnion(), n);
+  {
+    size_t b2r = 0;
+    thrust::counting_iterator<int> count(0);
+    auto rkey = thrust::make_transform_iterator(count, ReverseKey{key, n});
+    auto rbox = thrust::make_transform_iterator(count, ReverseBox{boxes, n});
+    cub::DeviceScan::InclusiveScanByKey(nullptr, b2r, rkey, rbox, pre0, BoxUnion(), n);
+    b2 = std::max(b2, b2r);
+  }
   cub::DeviceScan::ExclusiveSum(nullptr, b3, flags, lscan, std::max(n, cap));
   tmp_bytes = std::max(b1, std::max(b2, b3));
   size_t b4 = 0, b5 = 0;
@@ -1060,12 +1082,14 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
     }
     for (int a = 0; a < 3; ++a) {
       size_t tb = tmp_bytes;
-      k_gather_boxes<<<blocks(n), 256, 0, sm>>>(P, I.a[a], n, false, key, boxes, key_rev);
+      k_gather_boxes<<<blocks(n), 256, 0, sm>>>(P, I.a[a], n, boxes);
       cub::DeviceScan::InclusiveScanByKey(tmp, tb, key, boxes, pre_ax[a], BoxUnion(), n,
                                           cub::Equality(), sm);
-      k_gather_boxes<<<blocks(n), 256, 0, sm>>>(P, I.a[a], n, true, key, boxes, key_rev);
       tb = tmp_bytes;
-      cub::DeviceScan::InclusiveScanByKey(tmp, tb, key_rev, boxes, suf_ax[a], BoxUnion(), n,
+      thrust::counting_iterator<int> count(0);
+      auto rkey = thrust::make_transform_iterator(count, ReverseKey{key, n});
+      auto rbox = thrust::make_transform_iterator(count, ReverseBox{boxes, n});
+      cub::DeviceScan::InclusiveScanByKey(tmp, tb, rkey, rbox, suf_ax[a], BoxUnion(), n,
                                           cub::Equality(), sm);
     }
     costs(certify ? 1 : 0);
@@ -1122,7 +1146,7 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
     cudaError_t e = cudaStreamSynchronize(sm);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "BVH build levels");
     if (h[7] > 0)
-      k_subtrees<<<(unsigned)((h[7] + kSubtreeWarps - 1) / kSubtreeWarps), 32 * kSubtreeWarps, 0, sm>>>(
+      k_subtrees<<<(unsigned)h[7], kSubtreeThreads, 0, sm>>>(
           P, I, N, sub_roots, counters + 7, c.leaf_size, c.traversal, counters, counters + 2, side);
     cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, sm);
     e = cudaStreamSynchronize(sm);

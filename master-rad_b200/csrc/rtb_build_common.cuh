@@ -57,6 +57,7 @@ __device__ __forceinline__ unsigned long long order_key(double v) {
 struct Prims {
   float* lo[3];
   float* hi[3];
+  Box* box;          // the same bounds, one 24-byte record per primitive (gathers)
   double* cen[3];
   double* w;         // construction weight q = 1 + lambda (c - 1), or 1
   double* measured;  // c
@@ -104,11 +105,15 @@ __global__ void k_prims(const float* spheres, const float* boxes, const float* a
       hi[k] = up2(b[3 + k]);
     }
   }
+  Box bx;
   for (int k = 0; k < 3; ++k) {
     P.lo[k][p] = lo[k];
     P.hi[k][p] = hi[k];
     P.cen[k][p] = ((double)lo[k] + (double)hi[k]) * 0.5;
+    bx.mn[k] = lo[k];
+    bx.mx[k] = hi[k];
   }
+  P.box[p] = bx;
   double m = c.measured[t];
   P.measured[p] = m;
   P.w[p] = c.weighted ? 1.0 + c.lambda * (m - 1.0) : 1.0;
@@ -301,7 +306,7 @@ inline rtb_status build_setup(rtb_context* ctx, const rtb_scene_desc* desc, cons
   if (!desc || !cfg) return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "null argument");
   if (cfg->mode < 0 || cfg->mode > 7) return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "unknown BVH build mode");
   if (cfg->mode == 4 || cfg->mode == 5)
-    return fail(ctx, RTB_ERR_UNSUPPORTED, "SBVH build modes are not built on the device");
+    return fail(ctx, RTB_ERR_UNSUPPORTED, "the SBVH modes have their own builder (rtb_scene_build)");
   if (cfg->mode > 5 && !allow_rotations)
     return fail(ctx, RTB_ERR_UNSUPPORTED, "rotation modes apply to the full-sweep builder");
   if (cfg->leaf_size < 1) return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "BVH leaf size must be positive.");
@@ -337,6 +342,7 @@ inline Prims alloc_prims(Workspace& W, int n) {
     P.hi[k] = W.alloc<float>(n);
     P.cen[k] = W.alloc<double>(n);
   }
+  P.box = W.alloc<Box>(n);
   P.w = W.alloc<double>(n);
   P.measured = W.alloc<double>(n);
   P.ref = W.alloc<int>(n);

@@ -128,6 +128,10 @@ rtb_status build_bvh(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_bui
 rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_build_config* cfg,
                              const rtb_build_options* options, rtb_scene** out, rtb_bvh_stats* stats);
 
+// rtb_sbvh.cu: the SBVH modes (4, 5), built on the host in depth-first order.
+rtb_status build_bvh_sbvh(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_build_config* cfg,
+                          const rtb_build_options* options, rtb_scene** out, rtb_bvh_stats* stats);
+
 // rtb_binned.cu
 rtb_status build_bvh_binned(rtb_context* ctx, const rtb_scene_desc* desc, const rtb_build_config* cfg,
                             int bins, rtb_scene** out, rtb_bvh_stats* stats);

@@ -55,7 +55,8 @@ class BvhStats(C.Structure):
                 ("generalized_sah_cost", C.c_double), ("uniform_sah_cost", C.c_double),
                 ("weighted_sah_cost", C.c_double), ("bytes", C.c_longlong),
                 ("build_ms", C.c_double), ("sequential_nodes", C.c_int),
-                ("rotation_count", C.c_int)]
+                ("rotation_count", C.c_int), ("spatial_split_count", C.c_int),
+                ("duplicate_reference_count", C.c_int)]
 
 
 class BuildOptions(C.Structure):

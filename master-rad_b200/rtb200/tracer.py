@@ -45,7 +45,7 @@ BvhStats = collections.namedtuple("BvhStats", [
     "node_count", "root_count", "leaf_count", "max_depth", "primitive_ref_count", "leaf_size",
     "build_mode", "generalized_sah_cost", "uniform_sah_cost", "weighted_sah_cost", "bytes",
     "min_leaf_occupancy", "max_leaf_occupancy", "mean_leaf_occupancy", "build_ms",
-    "sequential_nodes", "rotation_count"])
+    "sequential_nodes", "rotation_count", "spatial_split_count", "duplicate_reference_count"])
 
 
 def validate_full_path_depth(max_depth: int) -> None:
@@ -169,7 +169,8 @@ class ResidentScene:
                          st.primitive_ref_count, st.leaf_size, cfg.mode.name,
                          st.generalized_sah_cost, st.uniform_sah_cost, st.weighted_sah_cost,
                          st.bytes, st.min_leaf_occupancy, st.max_leaf_occupancy, mean,
-                         st.build_ms, st.sequential_nodes, st.rotation_count)
+                         st.build_ms, st.sequential_nodes, st.rotation_count,
+                         st.spatial_split_count, st.duplicate_reference_count)
         return ResidentScene(ctx, h, stats)
 
     def download_bvh(self):

@@ -141,6 +141,45 @@ def build_bvh(scene, config=None, bins=0, rotation_passes=4):
     return out
 
 
+def build_bvh_sbvh(scene, config=None, options=None):
+    """The SBVH modes (UNIFORM_SBVH / WEIGHTED_SBVH): the restatement of the reference's
+    SpatialBuildState (oracle_bvh.cpp).  options: a BvhBuildOptions-like object (defaults
+    128 bins, multiplier 2.0, 8 splits per primitive, 16 references, overlap 1e-5).  The
+    Bvh's ``spatial_splits`` is BvhStats.spatialSplitCount."""
+    cfg = config if config is not None else scene.config
+    o = options if options is not None else scene.options
+    c = _Cfg(int(cfg.mode), cfg.leaf_size, cfg.traversal_weight, cfg.sphere_weight,
+             cfg.box_weight, cfg.affine_sphere_weight, cfg.affine_box_weight, cfg.lam)
+    ns, nb = scene.sphere_count, scene.box_count
+    nas, nab = scene.affine_sphere_count, scene.affine_box_count
+    n = ns + nb + nas + nab
+    cap = max(n, int(np.floor(n * o.max_reference_multiplier)), 1)
+    sp, bx = _f32(scene.sphere_data()), _f32(scene.box_data())
+    ab, bb = _f32(scene.affine_sphere_bounds()), _f32(scene.affine_box_bounds())
+    nbounds = np.zeros(2 * cap * 6, np.float32)
+    ndata = np.zeros(2 * cap * 4, np.int32)
+    refs = np.zeros(cap, np.int32)
+    roots = np.zeros(4, np.int32)
+    counts = np.zeros(7, np.int32)
+    sah = np.zeros(3, np.float64)
+    splits = C.c_int(0)
+    lib().orc_build_bvh_sbvh.restype = C.c_int
+    rc = lib().orc_build_bvh_sbvh(
+        _fp(sp), ns, _fp(bx), nb, _fp(ab), nas, _fp(bb), nab, C.byref(c), int(o.spatial_bins),
+        C.c_double(o.max_reference_multiplier), int(o.max_splits_per_primitive),
+        int(o.min_spatial_references), C.c_double(o.spatial_overlap_threshold), _fp(nbounds),
+        _ip(ndata), _ip(refs), _ip(roots), _ip(counts), sah.ctypes.data_as(C.POINTER(C.c_double)),
+        C.byref(splits))
+    if rc != 0:
+        raise RuntimeError("oracle SBVH build failed: %d" % rc)
+    nn, nr, nref = int(counts[0]), int(counts[1]), int(counts[4])
+    out = Bvh(nbounds[:6 * nn].copy(), ndata[:4 * nn].copy(), refs[:nref].copy(),
+              roots[:nr].copy(), counts, sah)
+    out.spatial_splits = splits.value
+    out.rotations = 0
+    return out
+
+
 def topology_sha256(node_bounds, node_data, refs, roots):
     h = hashlib.sha256()
     for arr in (np.asarray(node_bounds, np.float32).view(np.int32), np.asarray(node_data, np.int32),

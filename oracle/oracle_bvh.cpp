@@ -23,6 +23,12 @@
 //                           bottom-up, four candidates per node, recursive areaCost,
 //                           strict improvement by more than 1e-12, up to rotationPasses
 //                           passes while any rotation happened)
+//   * SpatialBuildState     gfxlab/gpu/GpuScene.java:1084-1412  (the SBVH modes: depth-first
+//                           recursion comparing the object split with the best of
+//                           spatialBins - 1 planes per axis, clipped duplicates under the
+//                           global budget floor(N * maxReferenceMultiplier), the greedy
+//                           unsplit pass over the split references in list order; leaves
+//                           collect the (clipped) references in visit order)
 // Arithmetic is IEEE double with no contraction (Java strictfp semantics); this file
 // must be compiled with -ffp-contract=off.
 //
@@ -524,6 +530,335 @@ double sah_cost(const std::vector<Node>& pool, int n, const std::vector<Prim>& p
   return (b.cfg.traversal + l) + r;
 }
 
+// ---- SpatialBuildState (GpuScene.java:1084-1412)
+struct SRef {
+  int ref;
+  int order;
+  Aabb bounds;
+  double measured;
+  int split_depth;
+};
+
+inline double sref_centroid(const SRef& r, int axis) { return (r.bounds.mn[axis] + r.bounds.mx[axis]) * 0.5; }
+
+// Record equality of SpatialReference (List.remove(Object) removes the first equal element).
+inline bool sref_equal(const SRef& a, const SRef& b) {
+  if (a.ref != b.ref || a.order != b.order || a.split_depth != b.split_depth) return false;
+  if (std::memcmp(&a.measured, &b.measured, 8) != 0) return false;
+  return std::memcmp(&a.bounds, &b.bounds, sizeof(Aabb)) == 0;
+}
+
+struct SpatialOptions {
+  int bins;
+  double max_reference_multiplier;
+  int max_splits_per_primitive;
+  int min_spatial_references;
+  double overlap_threshold;
+};
+
+struct ObjectSplit {
+  std::vector<SRef> sorted;
+  int left_count = 0;
+  double cost = 0.0;
+  Aabb left_bounds, right_bounds;
+  bool valid = false;
+};
+
+struct SpatialBuilder {
+  const Config& cfg;
+  SpatialOptions opt;
+  int max_refs;
+  int current;
+  int spatial_splits = 0;
+  std::vector<Node> pool;
+  std::vector<Prim> ordered;  // leaf references in visit order (clipped bounds)
+  static constexpr double EPS = 1.0e-12;
+
+  SpatialBuilder(const Config& c, const SpatialOptions& o, int n) : cfg(c), opt(o), current(n) {
+    max_refs = std::max(n, (int)std::floor((double)n * o.max_reference_multiplier));
+  }
+
+  double objective(const SRef& r) const {
+    if (!cfg.weighted) return 1.0;
+    double t = r.measured - 1.0;
+    t = cfg.lambda * t;
+    return 1.0 + t;
+  }
+
+  double weight_sum(const std::vector<SRef>& v) const {
+    double s = 0.0;
+    for (const SRef& r : v) s += objective(r);
+    return s;
+  }
+
+  static Aabb bounds_of(const std::vector<SRef>& v) {
+    Aabb b = v[0].bounds;
+    for (size_t i = 1; i < v.size(); ++i) b = unite(b, v[i].bounds);
+    return b;
+  }
+
+  int leaf(const Aabb& b, const std::vector<SRef>& refs) {
+    Node nd;
+    nd.bounds = b;
+    nd.start = (int)ordered.size();
+    for (const SRef& r : refs) {
+      Prim p{};
+      p.ref = r.ref;
+      p.order = r.order;
+      p.bounds = r.bounds;
+      p.measured = r.measured;
+      ordered.push_back(p);
+    }
+    nd.end = (int)ordered.size();
+    pool.push_back(nd);
+    return (int)pool.size() - 1;
+  }
+
+  ObjectSplit best_object_split(const std::vector<SRef>& refs, const Aabb& node_bounds) {
+    ObjectSplit best;
+    const int count = (int)refs.size();
+    for (int axis = 0; axis < 3; ++axis) {
+      std::vector<SRef> sorted = refs;
+      std::sort(sorted.begin(), sorted.end(), [axis](const SRef& a, const SRef& b) {
+        int cmp = java_double_compare(sref_centroid(a, axis), sref_centroid(b, axis));
+        return cmp != 0 ? cmp < 0 : a.order < b.order;
+      });
+      std::vector<Aabb> prefix(count), suffix(count);
+      std::vector<double> pw(count), sw(count);
+      prefix[0] = sorted[0].bounds;
+      pw[0] = objective(sorted[0]);
+      for (int i = 1; i < count; ++i) {
+        prefix[i] = unite(prefix[i - 1], sorted[i].bounds);
+        pw[i] = pw[i - 1] + objective(sorted[i]);
+      }
+      suffix[count - 1] = sorted[count - 1].bounds;
+      sw[count - 1] = objective(sorted[count - 1]);
+      for (int i = count - 2; i >= 0; --i) {
+        suffix[i] = unite(suffix[i + 1], sorted[i].bounds);
+        sw[i] = sw[i + 1] + objective(sorted[i]);
+      }
+      for (int i = 1; i < count; ++i) {
+        double cost = surface_area(node_bounds) * cfg.traversal;
+        cost = cost + surface_area(prefix[i - 1]) * pw[i - 1];
+        cost = cost + surface_area(suffix[i]) * sw[i];
+        if (!best.valid || cost < best.cost) {
+          best.valid = true;
+          best.sorted = sorted;
+          best.left_count = i;
+          best.cost = cost;
+          best.left_bounds = prefix[i - 1];
+          best.right_bounds = suffix[i];
+        }
+      }
+    }
+    return best;
+  }
+
+  bool should_attempt_spatial(const std::vector<SRef>& refs, const Aabb& node_bounds,
+                              const ObjectSplit& os) const {
+    if ((int)refs.size() < opt.min_spatial_references || current >= max_refs) return false;
+    Aabb ov;
+    bool empty = false;
+    for (int k = 0; k < 3; ++k) {
+      ov.mn[k] = std::max(os.left_bounds.mn[k], os.right_bounds.mn[k]);
+      ov.mx[k] = std::min(os.left_bounds.mx[k], os.right_bounds.mx[k]);
+    }
+    for (int k = 0; k < 3; ++k)
+      if (ov.mx[k] <= ov.mn[k]) empty = true;
+    double overlap = empty ? 0.0 : surface_area(ov);
+    return overlap / std::max(surface_area(node_bounds), 1.0e-30) > opt.overlap_threshold;
+  }
+
+  static Aabb clip_max(const Aabb& b, int axis, double v) {
+    Aabb r = b;
+    r.mx[axis] = std::min(b.mx[axis], v);
+    return r;
+  }
+  static Aabb clip_min(const Aabb& b, int axis, double v) {
+    Aabb r = b;
+    r.mn[axis] = std::max(b.mn[axis], v);
+    return r;
+  }
+
+  // best_plane: {axis, position}; false when no plane qualifies
+  bool best_spatial_plane(const std::vector<SRef>& refs, const Aabb& node_bounds, int* best_axis,
+                          double* best_pos) const {
+    bool found = false;
+    double best_cost = 0.0;
+    for (int axis = 0; axis < 3; ++axis) {
+      double lo = node_bounds.mn[axis], hi = node_bounds.mx[axis];
+      double extent = hi - lo;
+      if (!(extent > EPS)) continue;
+      for (int bin = 1; bin < opt.bins; ++bin) {
+        double plane = extent * (double)bin;
+        plane = plane / (double)opt.bins;
+        plane = lo + plane;
+        Aabb lb{}, rb{};
+        bool has_l = false, has_r = false;
+        double lw = 0.0, rw = 0.0;
+        int duplicates = 0;
+        for (const SRef& r : refs) {
+          if (r.bounds.mx[axis] <= plane + EPS) {
+            lb = has_l ? unite(lb, r.bounds) : r.bounds;
+            has_l = true;
+            lw += objective(r);
+          } else if (r.bounds.mn[axis] >= plane - EPS) {
+            rb = has_r ? unite(rb, r.bounds) : r.bounds;
+            has_r = true;
+            rw += objective(r);
+          } else if (r.split_depth < opt.max_splits_per_primitive) {
+            Aabb cl = clip_max(r.bounds, axis, plane), cr = clip_min(r.bounds, axis, plane);
+            lb = has_l ? unite(lb, cl) : cl;
+            rb = has_r ? unite(rb, cr) : cr;
+            has_l = has_r = true;
+            double w = objective(r);
+            lw += w;
+            rw += w;
+            duplicates++;
+          } else if (sref_centroid(r, axis) <= plane) {
+            lb = has_l ? unite(lb, r.bounds) : r.bounds;
+            has_l = true;
+            lw += objective(r);
+          } else {
+            rb = has_r ? unite(rb, r.bounds) : r.bounds;
+            has_r = true;
+            rw += objective(r);
+          }
+        }
+        if (!has_l || !has_r || current + duplicates > max_refs) continue;
+        double cost = surface_area(node_bounds) * cfg.traversal;
+        cost = cost + surface_area(lb) * lw;
+        cost = cost + surface_area(rb) * rw;
+        if (!found || cost < best_cost) {
+          found = true;
+          best_cost = cost;
+          *best_axis = axis;
+          *best_pos = plane;
+        }
+      }
+    }
+    return found;
+  }
+
+  static void remove_first_equal(std::vector<SRef>& v, const SRef& x) {
+    for (size_t i = 0; i < v.size(); ++i)
+      if (sref_equal(v[i], x)) {
+        v.erase(v.begin() + i);
+        return;
+      }
+  }
+
+  // partitionSpatial; false when a side would be empty
+  bool partition_spatial(const std::vector<SRef>& refs, int axis, double pos, std::vector<SRef>& left,
+                         std::vector<SRef>& right, int* duplicates) const {
+    struct Choice {
+      SRef original, l, r;
+    };
+    std::vector<Choice> choices;
+    for (const SRef& r : refs) {
+      double lo = r.bounds.mn[axis], hi = r.bounds.mx[axis];
+      if (hi <= pos + EPS) {
+        left.push_back(r);
+      } else if (lo >= pos - EPS) {
+        right.push_back(r);
+      } else if (r.split_depth < opt.max_splits_per_primitive) {
+        SRef lp = r, rp = r;
+        lp.bounds = clip_max(r.bounds, axis, pos);
+        lp.split_depth = r.split_depth + 1;
+        rp.bounds = clip_min(r.bounds, axis, pos);
+        rp.split_depth = r.split_depth + 1;
+        left.push_back(lp);
+        right.push_back(rp);
+        choices.push_back({r, lp, rp});
+      } else if (sref_centroid(r, axis) <= pos) {
+        left.push_back(r);
+      } else {
+        right.push_back(r);
+      }
+    }
+    if (left.empty() || right.empty()) return false;
+    for (const Choice& ch : choices) {
+      Aabb lb = bounds_of(left), rb = bounds_of(right);
+      double lw = weight_sum(left), rw = weight_sum(right);
+      double w = objective(ch.original);
+      double split_cost = surface_area(lb) * lw;
+      split_cost = split_cost + surface_area(rb) * rw;
+      double left_only = surface_area(unite(lb, ch.original.bounds)) * lw;
+      left_only = left_only + surface_area(rb) * std::max(0.0, rw - w);
+      double right_only = surface_area(lb) * std::max(0.0, lw - w);
+      right_only = right_only + surface_area(unite(rb, ch.original.bounds)) * rw;
+      if (left_only < split_cost && left_only <= right_only && right.size() > 1) {
+        remove_first_equal(left, ch.l);
+        remove_first_equal(right, ch.r);
+        left.push_back(ch.original);
+      } else if (right_only < split_cost && left.size() > 1) {
+        remove_first_equal(left, ch.l);
+        remove_first_equal(right, ch.r);
+        right.push_back(ch.original);
+      }
+    }
+    *duplicates = (int)(left.size() + right.size()) - (int)refs.size();
+    return true;
+  }
+
+  double split_cost(const std::vector<SRef>& left, const std::vector<SRef>& right,
+                    const Aabb& node_bounds) const {
+    double c = surface_area(node_bounds) * cfg.traversal;
+    c = c + surface_area(bounds_of(left)) * weight_sum(left);
+    c = c + surface_area(bounds_of(right)) * weight_sum(right);
+    return c;
+  }
+
+  int build(const std::vector<SRef>& refs) {
+    Aabb b = bounds_of(refs);
+    if (refs.size() == 1) return leaf(b, refs);
+    ObjectSplit os = best_object_split(refs, b);
+    std::vector<SRef> sl, sr;
+    bool have_spatial = false;
+    int dup = 0;
+    double spatial_cost = INFINITY;
+    if (should_attempt_spatial(refs, b, os)) {
+      int axis = 0;
+      double pos = 0.0;
+      if (best_spatial_plane(refs, b, &axis, &pos)) {
+        std::vector<SRef> cl, cr;
+        int d = 0;
+        if (partition_spatial(refs, axis, pos, cl, cr, &d) && current + d <= max_refs) {
+          spatial_cost = split_cost(cl, cr, b);
+          sl.swap(cl);
+          sr.swap(cr);
+          dup = d;
+          have_spatial = true;
+        }
+      }
+    }
+    double leaf_cost = surface_area(b) * weight_sum(refs);
+    bool choose_spatial = have_spatial && spatial_cost < os.cost;
+    double best_cost = choose_spatial ? spatial_cost : os.cost;
+    if ((int)refs.size() <= cfg.leaf_size && !(best_cost < leaf_cost)) return leaf(b, refs);
+    std::vector<SRef> left, right;
+    if (choose_spatial) {
+      left.swap(sl);
+      right.swap(sr);
+      current += dup;
+      spatial_splits++;
+    } else {
+      left.assign(os.sorted.begin(), os.sorted.begin() + os.left_count);
+      right.assign(os.sorted.begin() + os.left_count, os.sorted.end());
+    }
+    os.sorted.clear();
+    os.sorted.shrink_to_fit();
+    int l = build(left);
+    int r = build(right);
+    Node nd;
+    nd.bounds = b;
+    nd.left = l;
+    nd.right = r;
+    pool.push_back(nd);
+    return (int)pool.size() - 1;
+  }
+};
+
 Aabb float_box(float x0, float y0, float z0, float x1, float y1, float z1) {
   Aabb b;
   b.mn[0] = next_down2(x0);
@@ -550,39 +885,13 @@ typedef struct {
   double lambda;
 } orc_build_config;
 
-// Outputs must hold 2*N nodes (6 floats / 4 ints each), N refs and 4 roots, with
-// N = ns + nb + nas + nab.  counts: node_count, root_count, leaf_count, max_depth,
-// ref_count, min_leaf, max_leaf.  sah: generalized, uniform, weighted.
-// Returns 0 on success, negative on an unsupported configuration.
-static int build_any(const float* spheres, int ns, const float* boxes, int nb,
-                     const float* affine_sphere_bounds, int nas, const float* affine_box_bounds,
-                     int nab, const orc_build_config* cfg, int bins, int rotation_passes,
-                     float* node_bounds, int* node_data, int* refs, int* roots, int* counts,
-                     double* sah, int* rotations_out) {
-  bool rotations = cfg->mode == 6 || cfg->mode == 7;
-  if (cfg->mode < 0 || (cfg->mode > 3 && !rotations) || cfg->leaf_size < 1) return -1;
-  if (bins != 0 && (bins < 2 || bins > 32)) return -1;
-  if (rotations && (bins != 0 || rotation_passes < 1)) return -1;
-  bool weighted = cfg->mode == 1 || cfg->mode == 3 || cfg->mode == 7;
-  bool per_type = cfg->mode == 2 || cfg->mode == 3;
-  if (rotations_out) *rotations_out = 0;
-  Config c{weighted ? 1 : 0, cfg->leaf_size, cfg->traversal_weight,
-           weighted ? cfg->lambda : 0.0};
-  c.bins = bins;
-  {
-    const double measured[4] = {cfg->sphere_weight, cfg->box_weight, cfg->affine_sphere_weight,
-                                cfg->affine_box_weight};
-    for (int t = 0; t < 4; ++t) {
-      if (!weighted) continue;
-      double x = measured[t] - 1.0;
-      x = c.lambda * x;
-      c.type_weight[t] = 1.0 + x;
-    }
-  }
+// The bounded primitives in global order (spheres, boxes, affine spheres, affine boxes)
+// with their conservative bounds and centroids (GpuScene.java:626-649, 877-903).
+static std::vector<Prim> make_prims(const float* spheres, int ns, const float* boxes, int nb,
+                                    const float* affine_sphere_bounds, int nas,
+                                    const float* affine_box_bounds, int nab,
+                                    const orc_build_config* cfg) {
   int total = ns + nb + nas + nab;
-  std::memset(counts, 0, 7 * sizeof(int));
-  sah[0] = sah[1] = sah[2] = 0.0;
-  if (total == 0) return 0;
   std::vector<Prim> all;
   all.reserve(total);
   int order = 0;
@@ -625,6 +934,44 @@ static int build_any(const float* spheres, int ns, const float* boxes, int nb,
   }
   for (auto& p : all)
     for (int k = 0; k < 3; ++k) p.cen[k] = (p.bounds.mn[k] + p.bounds.mx[k]) * 0.5;
+  return all;
+}
+
+// Outputs must hold 2*N nodes (6 floats / 4 ints each), N refs and 4 roots, with
+// N = ns + nb + nas + nab.  counts: node_count, root_count, leaf_count, max_depth,
+// ref_count, min_leaf, max_leaf.  sah: generalized, uniform, weighted.
+// Returns 0 on success, negative on an unsupported configuration.
+static int build_any(const float* spheres, int ns, const float* boxes, int nb,
+                     const float* affine_sphere_bounds, int nas, const float* affine_box_bounds,
+                     int nab, const orc_build_config* cfg, int bins, int rotation_passes,
+                     float* node_bounds, int* node_data, int* refs, int* roots, int* counts,
+                     double* sah, int* rotations_out) {
+  bool rotations = cfg->mode == 6 || cfg->mode == 7;
+  if (cfg->mode < 0 || (cfg->mode > 3 && !rotations) || cfg->leaf_size < 1) return -1;
+  if (bins != 0 && (bins < 2 || bins > 32)) return -1;
+  if (rotations && (bins != 0 || rotation_passes < 1)) return -1;
+  bool weighted = cfg->mode == 1 || cfg->mode == 3 || cfg->mode == 7;
+  bool per_type = cfg->mode == 2 || cfg->mode == 3;
+  if (rotations_out) *rotations_out = 0;
+  Config c{weighted ? 1 : 0, cfg->leaf_size, cfg->traversal_weight,
+           weighted ? cfg->lambda : 0.0};
+  c.bins = bins;
+  {
+    const double measured[4] = {cfg->sphere_weight, cfg->box_weight, cfg->affine_sphere_weight,
+                                cfg->affine_box_weight};
+    for (int t = 0; t < 4; ++t) {
+      if (!weighted) continue;
+      double x = measured[t] - 1.0;
+      x = c.lambda * x;
+      c.type_weight[t] = 1.0 + x;
+    }
+  }
+  int total = ns + nb + nas + nab;
+  std::memset(counts, 0, 7 * sizeof(int));
+  sah[0] = sah[1] = sah[2] = 0.0;
+  if (total == 0) return 0;
+  std::vector<Prim> all = make_prims(spheres, ns, boxes, nb, affine_sphere_bounds, nas,
+                                     affine_box_bounds, nab, cfg);
 
   std::vector<std::vector<Prim>> parts;
   if (per_type) {
@@ -701,6 +1048,56 @@ int orc_build_bvh_binned(const float* spheres, int ns, const float* boxes, int n
   if (bins < 2 || bins > 32) return -1;
   return build_any(spheres, ns, boxes, nb, affine_sphere_bounds, nas, affine_box_bounds, nab, cfg,
                    bins, 4, node_bounds, node_data, refs, roots, counts, sah, nullptr);
+}
+
+// The SBVH modes (4 UNIFORM_SBVH, 5 WEIGHTED_SBVH) with BvhBuildOptions (spatialBins,
+// maxReferenceMultiplier, maxSplitsPerPrimitive, minSpatialReferences,
+// spatialOverlapThreshold).  Outputs must hold 2*R nodes and R refs, with
+// R = max(N, floor(N * maxReferenceMultiplier)); counts as orc_build_bvh's;
+// *spatial_splits receives BvhStats.spatialSplitCount.
+int orc_build_bvh_sbvh(const float* spheres, int ns, const float* boxes, int nb,
+                       const float* affine_sphere_bounds, int nas, const float* affine_box_bounds,
+                       int nab, const orc_build_config* cfg, int spatial_bins,
+                       double max_reference_multiplier, int max_splits_per_primitive,
+                       int min_spatial_references, double spatial_overlap_threshold,
+                       float* node_bounds, int* node_data, int* refs, int* roots, int* counts,
+                       double* sah, int* spatial_splits) {
+  if ((cfg->mode != 4 && cfg->mode != 5) || cfg->leaf_size < 1) return -1;
+  bool weighted = cfg->mode == 5;
+  Config c{weighted ? 1 : 0, cfg->leaf_size, cfg->traversal_weight, weighted ? cfg->lambda : 0.0};
+  std::memset(counts, 0, 7 * sizeof(int));
+  sah[0] = sah[1] = sah[2] = 0.0;
+  *spatial_splits = 0;
+  int total = ns + nb + nas + nab;
+  if (total == 0) return 0;
+  std::vector<Prim> all = make_prims(spheres, ns, boxes, nb, affine_sphere_bounds, nas,
+                                     affine_box_bounds, nab, cfg);
+  SpatialOptions o{spatial_bins, max_reference_multiplier, max_splits_per_primitive,
+                   min_spatial_references, spatial_overlap_threshold};
+  SpatialBuilder sb(c, o, total);
+  std::vector<SRef> initial(total);
+  for (int i = 0; i < total; ++i)
+    initial[i] = SRef{all[i].ref, all[i].order, all[i].bounds, all[i].measured, 0};
+  int root = sb.build(initial);
+  std::vector<Prim> dummy;
+  Builder stats_builder(dummy, c);
+  Summary s;
+  summarize(sb.pool, root, 0, s);
+  Flat f{node_bounds, node_data, refs};
+  roots[0] = flatten(sb.pool, root, sb.ordered, f);
+  sah[1] = sah_cost(sb.pool, root, sb.ordered, 0, stats_builder);
+  sah[2] = sah_cost(sb.pool, root, sb.ordered, 1, stats_builder);
+  sah[0] = sah_cost(sb.pool, root, sb.ordered, 2, stats_builder);
+  counts[0] = s.nodes;
+  counts[1] = 1;
+  counts[2] = s.leaves;
+  counts[3] = s.max_depth;
+  counts[4] = f.next_ref;
+  counts[5] = s.min_leaf == INT32_MAX ? 0 : s.min_leaf;
+  counts[6] = s.max_leaf;
+  *spatial_splits = sb.spatial_splits;
+  if (s.nodes != 2 * s.leaves - 1) return -2;
+  return 0;
 }
 
 }  // extern "C"

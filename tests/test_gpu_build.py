@@ -125,11 +125,13 @@ def test_device_build_degenerate_inputs(ctx):
     _check_identical(ctx, s2, s2.config)
 
 
-def test_device_build_rejects_unsupported_modes(ctx):
+def test_binned_build_rejects_the_sbvh_modes(ctx):
+    """The SBVH modes have their own builder (tests/test_gpu_sbvh.py); the binned object-SAH
+    builder refuses them."""
     scene = synth.hetero_scene(50, 1, synth.WORKLOAD_IDS["test"], 2)
     from rtb200 import native
     with pytest.raises(native.RtbError) as e:
-        ResidentScene.build(ctx, scene, BvhBuildConfig(BvhBuildMode.UNIFORM_SBVH, 4))
+        ResidentScene.build(ctx, scene, BvhBuildConfig(BvhBuildMode.UNIFORM_SBVH, 4), bins=16)
     assert e.value.status == 5
 
 

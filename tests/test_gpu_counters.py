@@ -6,9 +6,11 @@ Where the work does not depend on the tree walk the counts are equal: rays / pat
 plane tests and, in linear mode, every per-type primitive test.  In BVH mode this library
 walks its own 64-byte child-pair nodes (child boxes tested at the parent, leaves folded into
 it): its node visits are the reference's plus one per ray (the synthetic top node over the
-roots), and it tests a far leaf child even when the near leaf's hit already excludes it
-(about 5 % more primitive tests on the heterogeneous scene; skipping them measured slower,
-the check costs more inside the divergent leaf loop than the tests it saves)."""
+roots), plus the few that the postponed leaf tests do not prune (a lane keeps walking with
+its older, farther best hit while its leaves wait for the warp; bounded here at 3 %), and it
+tests a far leaf child even when the near leaf's hit already excludes it (about 5 % more
+primitive tests on the heterogeneous scene; skipping them measured slower, the check costs
+more inside the divergent leaf loop than the tests it saves)."""
 import dataclasses
 
 import numpy as np
@@ -64,14 +66,18 @@ def test_bvh_mode_counters_and_traversal_work(name):
         i = NAMES.index(k)
         assert ours[i] == ref[i], (k, ours[i], ref[i])
     assert ours[NAMES.index("overflow")] == 0 and ref[NAMES.index("overflow")] == 0
-    # node visits: the reference's, plus the synthetic top node once per ray (one root)
+    # node visits: the reference's, plus the synthetic top node once per ray (one root), plus
+    # those the postponed leaf tests leave unpruned
     i, r = NAMES.index("internal"), NAMES.index("rays")
-    assert abs(int(ours[i]) - int(ref[i]) - int(ours[r])) <= 0.001 * ref[i], (ours[i], ref[i], ours[r])
+    extra = int(ours[i]) - int(ref[i]) - int(ours[r])
+    print("\n%s: %d node visits beyond the reference's plus one per ray (%.3f %%)"
+          % (name, extra, 100.0 * extra / ref[i]))
+    assert -0.001 * ref[i] <= extra <= 0.03 * ref[i], (ours[i], ref[i], ours[r])
     # bounded-primitive tests: the same leaves reached, within the same order of magnitude
     p = NAMES.index("prim")
     ours_bvh = ours[p] - ours[NAMES.index("plane")]
     ref_bvh = ref[p] - ref[NAMES.index("plane")]
-    assert ref_bvh <= ours_bvh <= 1.1 * ref_bvh, (ours_bvh, ref_bvh)
+    assert ref_bvh <= ours_bvh <= 1.15 * ref_bvh, (ours_bvh, ref_bvh)
     work = frame_traversal_work(st)
     ref_work = traversal_work(*[ref[NAMES.index(k)] for k in
                                 ("aabb", "sphere", "box", "plane", "asphere", "abox")],
