@@ -445,13 +445,18 @@ __device__ __forceinline__ Box warp_bcast(const Box& b, int src) {
 }
 
 // Running sums of the 32 lanes' weights in lane order, continuing `acc`: lane q gets
-// acc + w_0 + ... + w_q added one by one (only the first `valid` lanes take part).
-__device__ __forceinline__ double warp_sequential_sum(double w, double& acc, int lane, int valid) {
+// acc + w_0 + ... + w_q added one by one.  Lanes past the node's end carry w = 0, and
+// adding +0 to a non-negative sum leaves it unchanged, so every chunk runs all 32 steps:
+// the 32 shuffles are issued ahead of the strictly sequential additions.
+__device__ __forceinline__ double warp_sequential_sum(double w, double& acc, int lane) {
+  double v[32];
+#pragma unroll
+  for (int q = 0; q < 32; ++q) v[q] = __shfl_sync(0xFFFFFFFFu, w, q);
   double mine = 0.0;
-  for (int q = 0; q < valid; ++q) {
-    double v = __shfl_sync(0xFFFFFFFFu, w, q);
-    acc = acc + v;
-    if (q == lane) mine = acc;
+#pragma unroll
+  for (int q = 0; q < 32; ++q) {
+    acc = acc + v[q];
+    mine = q == lane ? acc : mine;
   }
   return mine;
 }
@@ -508,11 +513,10 @@ __global__ void __launch_bounds__(kSubtreeThreads) k_subtrees(
       double acc = 0.0;
       for (int base = 0; base < m; base += 32) {
         int q = m - 1 - (base + lane);
-        int valid = min(32, m - base);
         Box b = q >= 0 ? prim_box(P, ix[q]) : empty_box();
         double w = q >= 0 ? P.w[ix[q]] : 0.0;
         b = BoxUnion()(warp_union_scan(b, lane), carry);
-        double sw = warp_sequential_sum(w, acc, lane, valid);
+        double sw = warp_sequential_sum(w, acc, lane);
         if (q >= 0) {
           sm.sbox[a][lo + q] = b;
           sm.sw[a][lo + q] = sw;
@@ -525,11 +529,10 @@ __global__ void __launch_bounds__(kSubtreeThreads) k_subtrees(
       acc = 0.0;
       for (int base = 0; base < m; base += 32) {
         int li = base + lane;
-        int valid = min(32, m - base);
         Box b = li < m ? prim_box(P, ix[li]) : empty_box();
         double w = li < m ? P.w[ix[li]] : 0.0;
         b = BoxUnion()(warp_union_scan(b, lane), carry);
-        double pw = warp_sequential_sum(w, acc, lane, valid);
+        double pw = warp_sequential_sum(w, acc, lane);
         int i = li + 1;  // split after li
         if (i < m) {
           double bl = surface_area(b) * pw;

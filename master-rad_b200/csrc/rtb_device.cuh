@@ -46,7 +46,10 @@ constexpr int kStackSize = 64;          // covers every tree depth the builders 
 // Leaf tests wait until at most this many lanes of the warp can still walk the tree
 // (measured on the 10k and 1M scenes: 4 was best of 0/4/8/12/16, 2 % above testing each
 // node's leaves at once).
-constexpr int kLeafPostponeLanes = 4;
+#ifndef RTB_LEAF_POSTPONE_LANES
+#define RTB_LEAF_POSTPONE_LANES 4
+#endif
+constexpr int kLeafPostponeLanes = RTB_LEAF_POSTPONE_LANES;
 
 enum PrimType { kSphere = 0, kBox = 1, kAffineSphere = 2, kAffineBox = 3, kPlane = 4 };
 
@@ -519,6 +522,32 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
     // can still walk, so the expensive primitive tests run with many lanes at once.  The
     // prune limits a lane uses while its leaves wait are from its older (farther) best
     // hit, which only visits more nodes, never fewer: the closest hit is unchanged.
+#ifdef RTB_SPECULATIVE
+    int pfirst0 = 0, pmeta0 = 0, pfirst1 = 0, pmeta1 = 0;
+    int qfirst0 = 0, qmeta0 = 0, qfirst1 = 0, qmeta1 = 0;
+    int npend = 0;
+    bool pend = false;  // this lane cannot take another leaf pair
+    while (__any_sync(0xFFFFFFFFu, node >= 0 || npend > 0)) {
+      pend = npend >= 2;
+      if (__popc(__ballot_sync(0xFFFFFFFFu, node >= 0 && !pend)) <= kLeafPostponeLanes &&
+          __any_sync(0xFFFFFFFFu, npend > 0)) {
+        int c0 = npend >= 1 ? (pmeta0 & 0xFFFFFF) : 0, c1 = npend >= 1 ? (pmeta1 & 0xFFFFFF) : 0;
+        int c2 = npend >= 2 ? (qmeta0 & 0xFFFFFF) : 0, c3 = npend >= 2 ? (qmeta1 & 0xFFFFFF) : 0;
+        int e1 = c0 + c1, e2 = e1 + c2, e3 = e2 + c3;
+        for (int k = 0; k < e3; ++k) {
+          int first, code, off;
+          if (k < c0) { first = pfirst0; code = pmeta0 >> 24; off = k; }
+          else if (k < e1) { first = pfirst1; code = pmeta1 >> 24; off = k - c0; }
+          else if (k < e2) { first = qfirst0; code = qmeta0 >> 24; off = k - e1; }
+          else { first = qfirst1; code = qmeta1 >> 24; off = k - e2; }
+          int ref = __ldg(S.refs + first + off);
+          int type = code == 4 ? (int)((unsigned)ref >> kTypeShift) : code;
+          test_ref<METRICS>(S, type, ref & kIndexMask, o, d, dd, b, c);
+        }
+        npend = 0;
+        continue;
+      }
+#else
     int pfirst0 = 0, pmeta0 = 0, pfirst1 = 0, pmeta1 = 0;
     bool pend = false;
     while (__any_sync(0xFFFFFFFFu, node >= 0 || pend)) {
@@ -536,6 +565,7 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
         pend = false;
         continue;
       }
+#endif
       if (node >= 0 && !pend) {
         const float4* np = S.nodes + 4 * node;
         float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2);
@@ -568,6 +598,22 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
             if (code1 == 4) c->mixed++; else c->homo++;
           }
         }
+#ifdef RTB_SPECULATIVE
+        if (count0 + count1 > 0) {
+          if (npend == 0) {
+            pfirst0 = first0;
+            pmeta0 = count0 | (code0 << 24);
+            pfirst1 = first1;
+            pmeta1 = count1 | (code1 << 24);
+          } else {
+            qfirst0 = first0;
+            qmeta0 = count0 | (code0 << 24);
+            qfirst1 = first1;
+            qmeta1 = count1 | (code1 << 24);
+          }
+          npend++;
+        }
+#else
         if (count0 + count1 > 0) {
           pend = true;
           pfirst0 = first0;
@@ -575,6 +621,7 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
           pfirst1 = first1;
           pmeta1 = count1 | (code1 << 24);
         }
+#endif
         float plim = prune_limit(b.t);
         int next = (hn && ln >= 0) ? ln : -1;
         if (hf && lf >= 0 && ef <= plim) {
