@@ -57,14 +57,14 @@ FALLBACK_HBM_GBS = 6650.0
 # dram__bytes_read.sum + dram__bytes_write.sum of k_render per sample, from one ncu capture
 # of the same scene at 1024x768x4 spp (profiles/k_render_hetero10k_1024x768x4spp_full.md);
 # workloads without a capture report null traffic.
-TRAFFIC_BYTES_PER_SAMPLE = {"hetero": (18.30e6 + 110.59e6) / 3145728}
-# smsp__inst_executed.sum of k_render per sample from the same capture (9.136 G warp
+TRAFFIC_BYTES_PER_SAMPLE = {"hetero": (26.58e6 + 143.07e6) / 3145728}
+# smsp__inst_executed.sum of k_render per sample from the same capture (8.862 G warp
 # instructions for 3,145,728 samples), for the issue bound: warp instructions per second
 # against one instruction per cycle on each of the 4 schedulers of every SM.
-INST_PER_SAMPLE = {"hetero": 9.136e9 / 3145728}
+INST_PER_SAMPLE = {"hetero": 8.862e9 / 3145728}
 # smsp__thread_inst_executed_per_inst_executed of the same capture: active lanes per warp
 # instruction, which scales the issue bound to lane-instructions doing useful work.
-LANES_PER_INST = {"hetero": 9.13}
+LANES_PER_INST = {"hetero": 9.22}
 
 
 def issue_roofline(workload, samples, launch_ms, sm_count, sm_mhz):

@@ -44,12 +44,8 @@ constexpr int kTypeShift = 30;
 constexpr int kIndexMask = 0x3FFFFFFF;  // K:20
 constexpr int kStackSize = 64;          // covers every tree depth the builders produce
 // Leaf tests wait until at most this many lanes of the warp can still walk the tree
-// (measured on the 10k and 1M scenes: 4 was best of 0/4/8/12/16, 2 % above testing each
-// node's leaves at once).
-#ifndef RTB_LEAF_POSTPONE_LANES
-#define RTB_LEAF_POSTPONE_LANES 4
-#endif
-constexpr int kLeafPostponeLanes = RTB_LEAF_POSTPONE_LANES;
+// (measured on the 10k and 1M scenes: 4 was best of 0/2/4/8/12/16).
+constexpr int kLeafPostponeLanes = 4;
 
 enum PrimType { kSphere = 0, kBox = 1, kAffineSphere = 2, kAffineBox = 3, kPlane = 4 };
 
@@ -486,11 +482,11 @@ __device__ __noinline__ void test_all_primitives(const DevScene& S, float3 o, fl
 //
 // Warp-cooperative: all 32 lanes of the warp call it together (lanes without a ray pass
 // active = false).  The traversal loop is warp-uniform -- each iteration every lane that
-// still walks processes one node: it tests both child boxes, records the (at most two)
-// leaf children it reached, then picks the next interior node; once at most
-// kLeafPostponeLanes lanes can still walk, the recorded leaves of all lanes are tested
-// together -- and the loop condition is a warp vote, so divergent lanes reconverge once per
-// node.  Every lane
+// still walks processes one node: it tests both child boxes, records the leaf children it
+// reached (a lane holds up to two recorded pairs, walking on after the first), then picks
+// the next interior node; once at most kLeafPostponeLanes lanes can still walk, the
+// recorded leaves of all lanes are tested together -- and the loop condition is a warp
+// vote, so divergent lanes reconverge once per node.  Every lane
 // takes part in the votes, also where lanes hold different scenes and only some of them
 // have a tree (the batch kernel's lanes may belong to different jobs).
 //
@@ -517,12 +513,12 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
     // A tree visits each node at most once per ray; the cap only matters for malformed
     // (cyclic) caller-supplied trees, which then take the exhaustive path.
     int budget = S.node_count + 8;
-    // Leaf postponing: a lane that reaches leaf children records them and stops walking;
-    // the warp tests the recorded leaves together once at most kLeafPostponeLanes lanes
-    // can still walk, so the expensive primitive tests run with many lanes at once.  The
-    // prune limits a lane uses while its leaves wait are from its older (farther) best
+    // Leaf postponing with speculative walking: a lane that reaches leaf children records
+    // them and walks on to its next leaf children (two recorded pairs at most, then it
+    // waits); the warp tests the recorded leaves together once at most kLeafPostponeLanes
+    // lanes can still walk, so the expensive primitive tests run with many lanes at once.
+    // The prune limits a lane uses while its leaves wait are from its older (farther) best
     // hit, which only visits more nodes, never fewer: the closest hit is unchanged.
-#ifdef RTB_SPECULATIVE
     int pfirst0 = 0, pmeta0 = 0, pfirst1 = 0, pmeta1 = 0;
     int qfirst0 = 0, qmeta0 = 0, qfirst1 = 0, qmeta1 = 0;
     int npend = 0;
@@ -535,11 +531,17 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
         int c2 = npend >= 2 ? (qmeta0 & 0xFFFFFF) : 0, c3 = npend >= 2 ? (qmeta1 & 0xFFFFFF) : 0;
         int e1 = c0 + c1, e2 = e1 + c2, e3 = e2 + c3;
         for (int k = 0; k < e3; ++k) {
-          int first, code, off;
-          if (k < c0) { first = pfirst0; code = pmeta0 >> 24; off = k; }
-          else if (k < e1) { first = pfirst1; code = pmeta1 >> 24; off = k - c0; }
-          else if (k < e2) { first = qfirst0; code = qmeta0 >> 24; off = k - e1; }
-          else { first = qfirst1; code = qmeta1 >> 24; off = k - e2; }
+          int first, meta, off;
+          if (k < c0) {
+            first = pfirst0, meta = pmeta0, off = k;
+          } else if (k < e1) {
+            first = pfirst1, meta = pmeta1, off = k - c0;
+          } else if (k < e2) {
+            first = qfirst0, meta = qmeta0, off = k - e1;
+          } else {
+            first = qfirst1, meta = qmeta1, off = k - e2;
+          }
+          int code = meta >> 24;
           int ref = __ldg(S.refs + first + off);
           int type = code == 4 ? (int)((unsigned)ref >> kTypeShift) : code;
           test_ref<METRICS>(S, type, ref & kIndexMask, o, d, dd, b, c);
@@ -547,25 +549,6 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
         npend = 0;
         continue;
       }
-#else
-    int pfirst0 = 0, pmeta0 = 0, pfirst1 = 0, pmeta1 = 0;
-    bool pend = false;
-    while (__any_sync(0xFFFFFFFFu, node >= 0 || pend)) {
-      if (__popc(__ballot_sync(0xFFFFFFFFu, node >= 0 && !pend)) <= kLeafPostponeLanes &&
-          __any_sync(0xFFFFFFFFu, pend)) {
-        int count0 = pend ? (pmeta0 & 0xFFFFFF) : 0, count1 = pend ? (pmeta1 & 0xFFFFFF) : 0;
-        int code0 = pmeta0 >> 24, code1 = pmeta1 >> 24;
-        for (int k = 0; k < count0 + count1; ++k) {
-          bool second = k >= count0;
-          int ref = __ldg(S.refs + (second ? pfirst1 + (k - count0) : pfirst0 + k));
-          int code = second ? code1 : code0;
-          int type = code == 4 ? (int)((unsigned)ref >> kTypeShift) : code;
-          test_ref<METRICS>(S, type, ref & kIndexMask, o, d, dd, b, c);
-        }
-        pend = false;
-        continue;
-      }
-#endif
       if (node >= 0 && !pend) {
         const float4* np = S.nodes + 4 * node;
         float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2);
@@ -598,7 +581,6 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
             if (code1 == 4) c->mixed++; else c->homo++;
           }
         }
-#ifdef RTB_SPECULATIVE
         if (count0 + count1 > 0) {
           if (npend == 0) {
             pfirst0 = first0;
@@ -613,15 +595,6 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
           }
           npend++;
         }
-#else
-        if (count0 + count1 > 0) {
-          pend = true;
-          pfirst0 = first0;
-          pmeta0 = count0 | (code0 << 24);
-          pfirst1 = first1;
-          pmeta1 = count1 | (code1 << 24);
-        }
-#endif
         float plim = prune_limit(b.t);
         int next = (hn && ln >= 0) ? ln : -1;
         if (hf && lf >= 0 && ef <= plim) {
