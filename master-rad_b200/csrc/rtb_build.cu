@@ -401,7 +401,15 @@ constexpr int kSubtreeSize = kSeqNodeSize;
 constexpr int kSubtreeThreads = 96;  // one warp per axis
 
 struct SubtreeSmem {
-  int idx[3][kSubtreeSize];     // the subtree's three axis orders
+  // The subtree's primitives get local slots 0..M-1 (axis 0's order at the root); the
+  // axis orders hold slots, and the primitives' boxes, weights and centroids are staged
+  // by slot, so the sweeps read shared memory only.
+  int gid[kSubtreeSize];        // slot -> primitive
+  Box lbox[kSubtreeSize];
+  double lw[kSubtreeSize];
+  double lcen[3][kSubtreeSize];
+  unsigned char lside[kSubtreeSize];
+  int idx[3][kSubtreeSize];     // the subtree's three axis orders (slots)
   Box sbox[3][kSubtreeSize];    // per axis: suffix boxes of the current node
   double sw[3][kSubtreeSize];   // per axis: suffix weights
   int tmp[3][kSubtreeSize];     // per axis: partition scratch
@@ -419,8 +427,6 @@ __device__ __forceinline__ Box empty_box() {
   }
   return b;
 }
-
-__device__ __forceinline__ Box prim_box(const Prims& P, int p) { return P.box[p]; }
 
 // Inclusive union over lanes 0..lane (min / max are exact in any order).
 __device__ __forceinline__ Box warp_union_scan(Box b, int lane) {
@@ -471,14 +477,24 @@ __device__ __forceinline__ bool lex_less(double c, long long f, double bc, long 
 // (or broadcast through shared memory), so the block's barriers are uniform.
 __global__ void __launch_bounds__(kSubtreeThreads) k_subtrees(
     const Prims P, IdxSet I, Nodes N, const int* roots, const int* root_count, int leaf_size,
-    double traversal, int* node_counter, int* stats, unsigned char* side) {
+    double traversal, int* node_counter, int* stats, int* slot_of) {
   __shared__ SubtreeSmem sm;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if ((int)blockIdx.x >= *root_count) return;
   const int root = roots[blockIdx.x];
   const int rs = N.start[root], re = N.end[root], M = re - rs;
-  for (int a = 0; a < 3; ++a)
-    for (int i = threadIdx.x; i < M; i += kSubtreeThreads) sm.idx[a][i] = I.a[a][rs + i];
+  for (int i = threadIdx.x; i < M; i += kSubtreeThreads) {
+    int p = I.a[0][rs + i];
+    sm.gid[i] = p;
+    sm.lbox[i] = P.box[p];
+    sm.lw[i] = P.w[p];
+    for (int a = 0; a < 3; ++a) sm.lcen[a][i] = P.cen[a][p];
+    slot_of[p] = i;  // each primitive belongs to one subtree
+    sm.idx[0][i] = i;
+  }
+  __syncthreads();
+  for (int a = 1; a < 3; ++a)
+    for (int i = threadIdx.x; i < M; i += kSubtreeThreads) sm.idx[a][i] = slot_of[I.a[a][rs + i]];
   if (threadIdx.x == 0) {
     sm.stack[0] = root;
     sm.sp = 1;
@@ -495,7 +511,7 @@ __global__ void __launch_bounds__(kSubtreeThreads) k_subtrees(
     const int oa = N.order_axis[node];
     // node bounds (every warp computes the same union)
     Box nb = empty_box();
-    for (int i = lane; i < m; i += 32) nb = BoxUnion()(nb, prim_box(P, sm.idx[0][lo + i]));
+    for (int i = lane; i < m; i += 32) nb = BoxUnion()(nb, sm.lbox[sm.idx[0][lo + i]]);
     for (int off = 16; off > 0; off >>= 1) {
       Box o;
       for (int k = 0; k < 3; ++k) {
@@ -510,14 +526,14 @@ __global__ void __launch_bounds__(kSubtreeThreads) k_subtrees(
     long long best_flat = 0x7FFFFFFFFFFFFFFFLL;
     const int a = warp;
     const int* ix = sm.idx[a] + lo;
-    if (m > 1 && P.cen[a][ix[m - 1]] - P.cen[a][ix[0]] > 1.0e-12) {
+    if (m > 1 && sm.lcen[a][ix[m - 1]] - sm.lcen[a][ix[0]] > 1.0e-12) {
       // suffix boxes and weights, from the last position down (GpuScene.java:1476-1480)
       Box carry = empty_box();
       double acc = 0.0;
       for (int base = 0; base < m; base += 32) {
         int q = m - 1 - (base + lane);
-        Box b = q >= 0 ? prim_box(P, ix[q]) : empty_box();
-        double w = q >= 0 ? P.w[ix[q]] : 0.0;
+        Box b = q >= 0 ? sm.lbox[ix[q]] : empty_box();
+        double w = q >= 0 ? sm.lw[ix[q]] : 0.0;
         b = BoxUnion()(warp_union_scan(b, lane), carry);
         double sw = warp_sequential_sum(w, acc, lane);
         if (q >= 0) {
@@ -532,8 +548,8 @@ __global__ void __launch_bounds__(kSubtreeThreads) k_subtrees(
       acc = 0.0;
       for (int base = 0; base < m; base += 32) {
         int li = base + lane;
-        Box b = li < m ? prim_box(P, ix[li]) : empty_box();
-        double w = li < m ? P.w[ix[li]] : 0.0;
+        Box b = li < m ? sm.lbox[ix[li]] : empty_box();
+        double w = li < m ? sm.lw[ix[li]] : 0.0;
         b = BoxUnion()(warp_union_scan(b, lane), carry);
         double pw = warp_sequential_sum(w, acc, lane);
         int i = li + 1;  // split after li
@@ -574,7 +590,7 @@ __global__ void __launch_bounds__(kSubtreeThreads) k_subtrees(
     bool leaf = m == 1 || best == CUDART_INF;
     if (!leaf && m <= leaf_size) {
       double wsum = 0.0;
-      for (int j = 0; j < m; ++j) wsum = wsum + P.w[oa < 0 ? s + j : sm.idx[oa][lo + j]];
+      for (int j = 0; j < m; ++j) wsum = wsum + (oa < 0 ? P.w[s + j] : sm.lw[sm.idx[oa][lo + j]]);
       if (!(best < surface_area(nb) * wsum)) leaf = true;
     }
     if (threadIdx.x == 0) {
@@ -613,7 +629,7 @@ __global__ void __launch_bounds__(kSubtreeThreads) k_subtrees(
     }
     // stable partition of the other two axis orders by side
     if (warp == axis)
-      for (int i = lane; i < m; i += 32) side[sm.idx[axis][lo + i]] = i >= pos ? 1 : 0;
+      for (int i = lane; i < m; i += 32) sm.lside[sm.idx[axis][lo + i]] = i >= pos ? 1 : 0;
     __syncthreads();
     if (warp != axis) {
       int* t = sm.tmp[a];
@@ -622,7 +638,7 @@ __global__ void __launch_bounds__(kSubtreeThreads) k_subtrees(
         int li = base + lane;
         bool in = li < m;
         int p = in ? sm.idx[a][lo + li] : 0;
-        bool left = in && side[p] == 0;
+        bool left = in && sm.lside[p] == 0;
         unsigned bal = __ballot_sync(0xFFFFFFFFu, left);
         if (left) t[nl + __popc(bal & ((1u << lane) - 1u))] = p;
         nl += __popc(bal);
@@ -632,7 +648,7 @@ __global__ void __launch_bounds__(kSubtreeThreads) k_subtrees(
         int li = base + lane;
         bool in = li < m;
         int p = in ? sm.idx[a][lo + li] : 0;
-        bool right = in && side[p] != 0;
+        bool right = in && sm.lside[p] != 0;
         unsigned bal = __ballot_sync(0xFFFFFFFFu, right);
         if (right) t[pos + nr + __popc(bal & ((1u << lane) - 1u))] = p;
         nr += __popc(bal);
@@ -643,7 +659,7 @@ __global__ void __launch_bounds__(kSubtreeThreads) k_subtrees(
     __syncthreads();
   }
   for (int a = 0; a < 3; ++a)
-    for (int i = threadIdx.x; i < M; i += kSubtreeThreads) I.a[a][rs + i] = sm.idx[a][i];
+    for (int i = threadIdx.x; i < M; i += kSubtreeThreads) I.a[a][rs + i] = sm.gid[sm.idx[a][i]];
   if (threadIdx.x == 0 && leaves > 0) {
     atomicAdd(stats + 0, leaves);
     atomicMin(stats + 1, min_occ);
@@ -1158,7 +1174,7 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
     if (e != cudaSuccess) return cuda_fail(ctx, e, "BVH build levels");
     if (h[7] > 0)
       k_subtrees<<<(unsigned)h[7], kSubtreeThreads, 0, sm>>>(
-          P, I, N, sub_roots, counters + 7, c.leaf_size, c.traversal, counters, counters + 2, side);
+          P, I, N, sub_roots, counters + 7, c.leaf_size, c.traversal, counters, counters + 2, flags);
     cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, sm);
     e = cudaStreamSynchronize(sm);
     if (e == cudaSuccess) e = cudaGetLastError();

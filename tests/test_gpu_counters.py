@@ -9,8 +9,9 @@ it): its node visits are the reference's plus one per ray (the synthetic top nod
 roots), plus the few that the postponed leaf tests do not prune (a lane keeps walking with
 its older, farther best hit while its leaves wait and walks on speculatively; measured 1.1 % on
 the plain scene and 6.8 % on the heterogeneous one, bounded here at 10 %), and it
-tests a far leaf child even when the near leaf's hit already excludes it (about 5 % more
-primitive tests on the heterogeneous scene; skipping them measured slower, the check costs
+tests a far leaf child even when the near leaf's hit already excludes it, and the leaves the
+speculative walk reaches before the warp tests (16 % more primitive tests on the
+heterogeneous scene, bounded at 25 %; skipping far leaves measured slower, the check costs
 more inside the divergent leaf loop than the tests it saves)."""
 import dataclasses
 
@@ -78,7 +79,9 @@ def test_bvh_mode_counters_and_traversal_work(name):
     p = NAMES.index("prim")
     ours_bvh = ours[p] - ours[NAMES.index("plane")]
     ref_bvh = ref[p] - ref[NAMES.index("plane")]
-    assert ref_bvh <= ours_bvh <= 1.15 * ref_bvh, (ours_bvh, ref_bvh)
+    print("%s: bounded-primitive tests %d against the reference's %d (%.3f)"
+          % (name, ours_bvh, ref_bvh, ours_bvh / ref_bvh))
+    assert ref_bvh <= ours_bvh <= 1.25 * ref_bvh, (ours_bvh, ref_bvh)
     work = frame_traversal_work(st)
     ref_work = traversal_work(*[ref[NAMES.index(k)] for k in
                                 ("aabb", "sphere", "box", "plane", "asphere", "abox")],
