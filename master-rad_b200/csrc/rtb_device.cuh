@@ -45,7 +45,10 @@ constexpr int kIndexMask = 0x3FFFFFFF;  // K:20
 constexpr int kStackSize = 64;          // covers every tree depth the builders produce
 // Leaf tests wait until at most this many lanes of the warp can still walk the tree
 // (measured on the 10k and 1M scenes: 4 was best of 0/2/4/8/12/16).
-constexpr int kLeafPostponeLanes = 4;
+#ifndef RTB_LEAF_POSTPONE_LANES
+#define RTB_LEAF_POSTPONE_LANES 4
+#endif
+constexpr int kLeafPostponeLanes = RTB_LEAF_POSTPONE_LANES;
 
 enum PrimType { kSphere = 0, kBox = 1, kAffineSphere = 2, kAffineBox = 3, kPlane = 4 };
 

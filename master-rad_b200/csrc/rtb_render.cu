@@ -67,8 +67,11 @@ __device__ __forceinline__ uint32_t pixel_base_seed(unsigned long long frame_see
 // scenes far larger than the caches: there the local-memory stack's lines compete with the
 // scene for L1 and L2.  A scene that the caches hold keeps the whole stack in local memory
 // and the caches for itself.
+#ifndef RTB_RENDER_BLOCKS_PER_SM
+#define RTB_RENDER_BLOCKS_PER_SM 8  // 64 registers a thread; 7 and 6 measured slower
+#endif
 template <bool METRICS, int SDEPTH>
-__global__ void __launch_bounds__(128, 8) k_render(RenderArgs a) {
+__global__ void __launch_bounds__(128, RTB_RENDER_BLOCKS_PER_SM) k_render(RenderArgs a) {
   __shared__ int2 s_stack[SDEPTH > 0 ? SDEPTH : 1][128];
   const DevScene& S = a.S;
   const int lane = threadIdx.x & 31;
