@@ -27,9 +27,6 @@
 //    node's current order)) uses the parent's split-axis order, which is the order the
 //    Java primitives array holds when build() reaches the node.
 // The file is compiled with -fmad=false: no double expression is contracted.
-#include <thrust/iterator/counting_iterator.h>
-#include <thrust/iterator/transform_iterator.h>
-
 #include "rtb_build_common.cuh"
 
 namespace rtb {
@@ -47,24 +44,6 @@ __global__ void k_type_keys(const Prims P, const int* idx, int n, int* keys) {
   if (j < n) keys[j] = P.type[idx[j]];
 }
 
-
-// The primitives' boxes in one axis order (the suffix scan reads the same array backwards).
-__global__ void k_gather_boxes(const Prims P, const int* idx, int n, Box* out) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j < n) out[j] = P.box[idx[j]];
-}
-
-// Position j of the reversed order: element n - 1 - j (input iterators for the suffix scans).
-struct ReverseBox {
-  const Box* a;
-  int n;
-  __host__ __device__ __forceinline__ Box operator()(int j) const { return a[n - 1 - j]; }
-};
-struct ReverseKey {
-  const int* a;
-  int n;
-  __host__ __device__ __forceinline__ int operator()(int j) const { return a[n - 1 - j]; }
-};
 
 __global__ void k_gather_weights(const Prims P, const int* idx, int n, double* wpos) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -158,24 +137,6 @@ constexpr int kSeqNodeSize = 256;
 struct TypeCounts {
   unsigned long long a, b;  // (sphere | box << 32), (affine sphere | affine box << 32)
 };
-struct CountsAdd {
-  __device__ __forceinline__ TypeCounts operator()(const TypeCounts& x, const TypeCounts& y) const {
-    return TypeCounts{x.a + y.a, x.b + y.b};
-  }
-};
-
-__global__ void k_type_onehot(const Prims P, const int* idx, int n, TypeCounts* out) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  int t = P.type[idx[j]];
-  unsigned long long one = 1ULL << (32 * (t & 1));
-  out[j] = t < 2 ? TypeCounts{one, 0ULL} : TypeCounts{0ULL, one};
-}
-
-__device__ __forceinline__ TypeCounts counts_sub(TypeCounts x, TypeCounts y) {
-  return TypeCounts{x.a - y.a, x.b - y.b};
-}
-
 // sum_t c_t w_t, exact in double-double, rounded once: within one rounding of the true sum.
 __device__ __forceinline__ double counts_weight(TypeCounts c, const double* wt) {
   double cnt[4] = {(double)(c.a & 0xFFFFFFFFULL), (double)(c.a >> 32), (double)(c.b & 0xFFFFFFFFULL),
@@ -197,52 +158,299 @@ struct TypeWeights {
   double w[4];
 };
 
-__global__ void k_weights_counts(const Nodes N, const int* key, const int* level_of, int level, int n,
-                                 const TypeCounts* scan, TypeWeights W, double* pw, double* sw) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  int node = key[j];
-  if (level_of[node] != level) return;
-  int s = N.start[node], e = N.end[node];
-  if (e - s <= kSeqNodeSize) return;
-  TypeCounts total = scan[e - 1];
-  TypeCounts upto = scan[j];
-  pw[j] = counts_weight(upto, W.w);
-  TypeCounts before = j > s ? scan[j - 1] : TypeCounts{0ULL, 0ULL};
-  sw[j] = counts_weight(counts_sub(total, before), W.w);
+// ---- segmented scans over node-sorted positions
+//
+// The positions are sorted by node (key[j]), every node one contiguous segment.  For every
+// position j of a node at the current level, the forward scan gives the combination of the
+// values over [start of j's node, j] and the backward scan over [j, end of j's node].  Three
+// launches cover all three axes: every chunk of kSegChunk positions reduces to its partial
+// aggregates in both directions (k_seg_chunks); one block per (axis, direction) carries
+// them across the chunks (k_seg_carries); every chunk then scans again with its carries and
+// hands each position's results to a consumer (k_seg_apply) that evaluates the split costs
+// or the count-based weights in place, so no scanned array is written.  Chunks holding no
+// position of a node at the current level do no work (a node at the level never spans
+// such a chunk).  Box unions (min / max) and integer sums are exact, so any association of
+// them gives the sequential result bit for bit.
+constexpr int kSegThreads = 256, kSegItems = 4, kSegChunk = kSegThreads * kSegItems;
+constexpr int kSegWarps = kSegThreads / 32, kCarryThreads = 1024;
+
+template <class V>
+struct Seg {
+  int flag;  // a segment starts inside the span (in scan order): v starts there
+  V v;
+};
+
+template <bool DOWN, class V>
+__device__ __forceinline__ V shfl_v(V x, int d) {
+  static_assert(sizeof(V) % 4 == 0, "values of whole words");
+  constexpr int kWords = sizeof(V) / 4;
+  int w[kWords];
+  memcpy(w, &x, sizeof(V));
+#pragma unroll
+  for (int q = 0; q < kWords; ++q)
+    w[q] = DOWN ? __shfl_down_sync(0xFFFFFFFFu, w[q], d) : __shfl_up_sync(0xFFFFFFFFu, w[q], d);
+  memcpy(&x, w, sizeof(V));
+  return x;
 }
 
-// Split cost of every position (GpuScene.java:1482-1485).  cost[j] is the cost of putting
-// positions [s, j) left; +inf marks positions that are not candidates.  For nodes whose
-// weights came from counts, bound[j] limits |cost[j] - the reference's cost|.
-__global__ void k_costs(const Prims P, const int* idx, const Nodes N, const int* key,
-                        const int* level_of, int level, int axis, int n, const Box* pre,
-                        const Box* suf_rev, const double* pw, const double* sw, double traversal,
-                        int certified, double* cost, double* bound) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  int node = key[j];
-  double c = CUDART_INF;
-  int s = N.start[node], e = N.end[node];
-  if (level_of[node] == level && j > s && e - s > 1) {
-    double ext = P.cen[axis][idx[e - 1]] - P.cen[axis][idx[s]];
-    if (ext > 1.0e-12) {
-      Box node_box = pre[e - 1];
-      double a = surface_area(node_box) * traversal;
-      double al = surface_area(pre[j - 1]);
-      double ar = surface_area(suf_rev[n - 1 - j]);
-      double b = al * pw[j - 1];
-      double d = ar * sw[j];
-      c = (a + b) + d;
-      if (certified && e - s > kSeqNodeSize) {
-        const double u = 0x1p-53;
-        double kl = (double)(j - s), kr = (double)(e - j);
-        bound[j] = 2.0 * (al * pw[j - 1] * (kl * u) + ar * sw[j] * (kr * u) + 8.0 * u * c);
-      }
+// Segmented scan of a block's items in scan order: thread by thread, ITEMS consecutive
+// positions each; REV runs from the block's last position down.  flag[i] marks the first
+// position of a segment in scan order.  before[i] / incl[i] combine the segment's values up
+// to item i, excluding / including it, with `carry` standing for all positions ahead of
+// the block.  Returns the block's own aggregate (carry left out).
+template <class O, bool REV, int ITEMS, int WARPS>
+__device__ __forceinline__ Seg<typename O::V> seg_scan_block(const int (&flag)[ITEMS],
+                                                             const typename O::V (&v)[ITEMS],
+                                                             typename O::V carry,
+                                                             typename O::V (&before)[ITEMS],
+                                                             typename O::V (&incl)[ITEMS],
+                                                             Seg<typename O::V>* s_warp) {
+  using V = typename O::V;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int tf = 0;
+  V tv = O::identity();
+#pragma unroll
+  for (int q = 0; q < ITEMS; ++q) {
+    const int i = REV ? ITEMS - 1 - q : q;
+    tv = flag[i] ? v[i] : O::combine(tv, v[i]);
+    tf |= flag[i];
+  }
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    int of = REV ? __shfl_down_sync(0xFFFFFFFFu, tf, d) : __shfl_up_sync(0xFFFFFFFFu, tf, d);
+    V ov = shfl_v<REV>(tv, d);
+    if (REV ? lane + d < 32 : lane >= d) {
+      if (!tf) tv = O::combine(ov, tv);
+      tf |= of;
     }
   }
-  cost[j] = c;
+  int ef = REV ? __shfl_down_sync(0xFFFFFFFFu, tf, 1) : __shfl_up_sync(0xFFFFFFFFu, tf, 1);
+  V ev = shfl_v<REV>(tv, 1);
+  if (REV ? lane == 31 : lane == 0) {
+    ef = 0;
+    ev = O::identity();
+  }
+  if (REV ? lane == 0 : lane == 31) s_warp[w] = Seg<V>{tf, tv};
+  __syncthreads();
+  V acc = carry;
+  Seg<V> agg{0, O::identity()};
+  for (int q = 0; q < WARPS; ++q) {
+    const int u = REV ? WARPS - 1 - q : q;
+    const Seg<V> s = s_warp[u];
+    if (REV ? u > w : u < w) acc = s.flag ? s.v : O::combine(acc, s.v);
+    agg.v = s.flag ? s.v : O::combine(agg.v, s.v);
+    agg.flag |= s.flag;
+  }
+  V run = ef ? ev : O::combine(acc, ev);
+#pragma unroll
+  for (int q = 0; q < ITEMS; ++q) {
+    const int i = REV ? ITEMS - 1 - q : q;
+    before[i] = run;
+    run = flag[i] ? v[i] : O::combine(run, v[i]);
+    incl[i] = run;
+  }
+  __syncthreads();  // s_warp is free again
+  return agg;
 }
+
+// One thread's kSegItems positions from j0: segment starts (head) and ends (tail), node
+// ids, and values (the identity outside the loader's active nodes); bit i of the result is
+// set when position j0 + i is active.  Positions past n are segments of their own.
+template <class L>
+__device__ __forceinline__ int seg_load(const L& load, const int* key, int n, int a, int j0,
+                                        int (&head)[kSegItems], int (&tail)[kSegItems],
+                                        int (&node)[kSegItems], typename L::V (&v)[kSegItems]) {
+  int act = 0;
+  int kp = j0 > 0 && j0 <= n ? key[j0 - 1] : -1;
+#pragma unroll
+  for (int i = 0; i < kSegItems; ++i) {
+    const int j = j0 + i;
+    const int kj = j < n ? key[j] : -1;
+    const int kn = j + 1 < n ? key[j + 1] : -1;
+    node[i] = kj;
+    head[i] = j >= n || j == 0 || kj != kp;
+    tail[i] = j >= n || j == n - 1 || kj != kn;
+    const bool on = j < n && load.active(kj);
+    v[i] = on ? load(a, j) : L::identity();
+    act |= (int)on << i;
+    kp = kj;
+  }
+  return act;
+}
+
+// Per (chunk, axis): the chunk's aggregate in both directions.
+template <class L>
+__global__ void __launch_bounds__(kSegThreads) k_seg_chunks(const L load, const int* key, int n, int nc,
+                                                            Seg<typename L::V>* fwd,
+                                                            Seg<typename L::V>* bwd) {
+  using V = typename L::V;
+  __shared__ Seg<V> s_warp[kSegWarps];
+  const int a = blockIdx.y, c = blockIdx.x;
+  const int j0 = c * kSegChunk + threadIdx.x * kSegItems;
+  int head[kSegItems], tail[kSegItems], node[kSegItems];
+  V v[kSegItems], before[kSegItems], incl[kSegItems];
+  const int act = seg_load(load, key, n, a, j0, head, tail, node, v);
+  const size_t slot = (size_t)a * nc + c;
+  if (!__syncthreads_or(act)) {
+    if (threadIdx.x == 0) fwd[slot] = bwd[slot] = Seg<V>{1, L::identity()};
+    return;
+  }
+  Seg<V> af = seg_scan_block<L, false, kSegItems, kSegWarps>(head, v, L::identity(), before, incl, s_warp);
+  Seg<V> ab = seg_scan_block<L, true, kSegItems, kSegWarps>(tail, v, L::identity(), before, incl, s_warp);
+  if (threadIdx.x == 0) {
+    fwd[slot] = af;
+    bwd[slot] = ab;
+  }
+}
+
+// Per (axis, direction): chunk aggregates scanned in place over all chunks, 1024 at a time
+// with a running carry; afterwards fwd[c] holds the forward result at chunk c's last
+// position and bwd[c] the backward result at its first.
+template <class O>
+__global__ void __launch_bounds__(kCarryThreads) k_seg_carries(int nc, Seg<typename O::V>* fwd,
+                                                               Seg<typename O::V>* bwd) {
+  using V = typename O::V;
+  __shared__ Seg<V> s_warp[kCarryThreads / 32];
+  const bool rev = blockIdx.y != 0;
+  Seg<V>* s = (rev ? bwd : fwd) + (size_t)blockIdx.x * nc;
+  V carry = O::identity();
+  const int tiles = (nc + kCarryThreads - 1) / kCarryThreads;
+  for (int t = 0; t < tiles; ++t) {
+    const int c = (rev ? tiles - 1 - t : t) * kCarryThreads + threadIdx.x;
+    const Seg<V> x = c < nc ? s[c] : Seg<V>{1, O::identity()};
+    int flag[1] = {x.flag};
+    V v[1] = {x.v}, before[1], incl[1];
+    Seg<V> agg = rev ? seg_scan_block<O, true, 1, kCarryThreads / 32>(flag, v, carry, before, incl, s_warp)
+                     : seg_scan_block<O, false, 1, kCarryThreads / 32>(flag, v, carry, before, incl, s_warp);
+    if (c < nc) s[c] = Seg<V>{x.flag, incl[0]};
+    carry = agg.flag ? agg.v : O::combine(carry, agg.v);
+  }
+}
+
+// Per (chunk, axis): both scans with the carries, each active position handed to `use`.
+template <class L, class U>
+__global__ void __launch_bounds__(kSegThreads) k_seg_apply(const L load, const U use, const int* key, int n,
+                                                           int nc, const Seg<typename L::V>* fwd,
+                                                           const Seg<typename L::V>* bwd) {
+  using V = typename L::V;
+  __shared__ Seg<V> s_warp[kSegWarps];
+  const int a = blockIdx.y, c = blockIdx.x;
+  const int j0 = c * kSegChunk + threadIdx.x * kSegItems;
+  int head[kSegItems], tail[kSegItems], node[kSegItems];
+  V v[kSegItems], fb[kSegItems], fi[kSegItems], bb[kSegItems], bi[kSegItems];
+  const int act = seg_load(load, key, n, a, j0, head, tail, node, v);
+  if (!__syncthreads_or(act)) return;
+  const size_t slot = (size_t)a * nc + c;
+  const V cf = c > 0 ? fwd[slot - 1].v : L::identity();
+  const V cb = c + 1 < nc ? bwd[slot + 1].v : L::identity();
+  seg_scan_block<L, false, kSegItems, kSegWarps>(head, v, cf, fb, fi, s_warp);
+  seg_scan_block<L, true, kSegItems, kSegWarps>(tail, v, cb, bb, bi, s_warp);
+#pragma unroll
+  for (int i = 0; i < kSegItems; ++i)
+    if (act >> i & 1) use(a, j0 + i, node[i], tail[i], fb[i], fi[i], bi[i]);
+}
+
+struct BoxOp {
+  using V = Box;
+  __device__ static Box identity() {
+    Box b;
+    for (int k = 0; k < 3; ++k) {
+      b.mn[k] = CUDART_INF_F;
+      b.mx[k] = -CUDART_INF_F;
+    }
+    return b;
+  }
+  __device__ static Box combine(const Box& x, const Box& y) { return BoxUnion()(x, y); }
+};
+
+struct CountOp {
+  using V = TypeCounts;
+  __device__ static TypeCounts identity() { return TypeCounts{0ULL, 0ULL}; }
+  __device__ static TypeCounts combine(const TypeCounts& x, const TypeCounts& y) {
+    return TypeCounts{x.a + y.a, x.b + y.b};
+  }
+};
+
+// Primitive boxes in each axis order, for the nodes at the level.
+struct BoxLoad : BoxOp {
+  Prims P;
+  IdxSet I;
+  const int* level_of;
+  int level;
+  __device__ bool active(int node) const { return level_of[node] == level; }
+  __device__ Box operator()(int a, int j) const { return P.box[I.a[a][j]]; }
+};
+
+// One-hot type counts in each axis order, for the level's nodes above kSeqNodeSize.
+struct CountLoad : CountOp {
+  Prims P;
+  IdxSet I;
+  Nodes N;
+  const int* level_of;
+  int level;
+  __device__ bool active(int node) const {
+    return level_of[node] == level && N.end[node] - N.start[node] > kSeqNodeSize;
+  }
+  __device__ TypeCounts operator()(int a, int j) const {
+    int t = P.type[I.a[a][j]];
+    unsigned long long one = 1ULL << (32 * (t & 1));
+    return t < 2 ? TypeCounts{one, 0ULL} : TypeCounts{0ULL, one};
+  }
+};
+
+// Count-based prefix and suffix weights of every position of a large node.
+struct CountWeights {
+  TypeWeights tw;
+  double* pw[3];
+  double* sw[3];
+  __device__ void operator()(int a, int j, int, int, const TypeCounts&, const TypeCounts& upto,
+                             const TypeCounts& from) const {
+    pw[a][j] = counts_weight(upto, tw.w);
+    sw[a][j] = counts_weight(from, tw.w);
+  }
+};
+
+// Split cost of every position (GpuScene.java:1482-1485): cost[j] is the cost of putting
+// positions [s, j) left; +inf marks positions that are not candidates.  The left bounds
+// are the forward scan before j, the right bounds the backward scan at j, and the node's
+// bounds their union (written once per node, at its last position, for the axis-0 pass).
+// For nodes whose weights came from counts, bound[j] limits |cost[j] - the reference's cost|.
+struct SplitCosts {
+  Prims P;
+  IdxSet I;
+  Nodes N;
+  const double* pw[3];
+  const double* sw[3];
+  double traversal;
+  int certified;
+  double* cost[3];
+  double* bound[3];
+  Box* node_box;  // node bounds at each node's last position
+  __device__ void operator()(int a, int j, int node, int tail, const Box& left, const Box& upto,
+                             const Box& right) const {
+    if (a == 0 && tail) node_box[j] = upto;
+    int s = N.start[node], e = N.end[node];
+    double c = CUDART_INF;
+    if (j > s && e - s > 1) {
+      const int* idx = I.a[a];
+      double ext = P.cen[a][idx[e - 1]] - P.cen[a][idx[s]];
+      if (ext > 1.0e-12) {
+        double an = surface_area(BoxUnion()(left, right)) * traversal;
+        double al = surface_area(left);
+        double ar = surface_area(right);
+        double b = al * pw[a][j - 1];
+        double d = ar * sw[a][j];
+        c = (an + b) + d;
+        if (certified && e - s > kSeqNodeSize) {
+          const double u = 0x1p-53;
+          double kl = (double)(j - s), kr = (double)(e - j);
+          bound[a][j] = 2.0 * (al * pw[a][j - 1] * (kl * u) + ar * sw[a][j] * (kr * u) + 8.0 * u * c);
+        }
+      }
+    }
+    cost[a][j] = c;
+  }
+};
 
 // Nodes of this level split into those summed sequentially (small) and those certified.
 __global__ void k_split_lists(const Nodes N, const int* active, int k, int* small, int* small_count,
@@ -681,7 +889,7 @@ __global__ void k_depth_scatter(const Nodes N, int count, int* cursor, int* all_
 
 // Leaf-or-split decision per active node (GpuScene.java:1424-1447).
 __global__ void k_decide(const Prims P, IdxSet I, Nodes N, const int* active, int k,
-                         const double* best_cost, const long long* best_flat, const Box* pre0,
+                         const double* best_cost, const long long* best_flat, const Box* node_box,
                          int leaf_size, int* node_counter, int* next_active, int* next_count,
                          int* level_of, int level, int* stats, int* largest_child, int* small_roots,
                          int* small_count) {
@@ -690,7 +898,7 @@ __global__ void k_decide(const Prims P, IdxSet I, Nodes N, const int* active, in
   int node = active[g];
   int s = N.start[node], e = N.end[node];
   int n = e - s;
-  Box bounds = pre0[e - 1];
+  Box bounds = node_box[e - 1];
   N.bounds[node] = bounds;
   N.split_axis[node] = -1;
   bool leaf = n == 1 || best_cost[g] == CUDART_INF;
@@ -939,14 +1147,12 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
   Nodes N = alloc_nodes(W, cap);
   int* level_of = W.alloc<int>(cap);
   int* key = W.alloc<int>(n);
-  Box* boxes = W.alloc<Box>(n);
-  Box* pre_ax[3];
-  Box* suf_ax[3];
-  for (int a = 0; a < 3; ++a) {
-    pre_ax[a] = W.alloc<Box>(n);
-    suf_ax[a] = W.alloc<Box>(n);
-  }
-  Box* pre0 = pre_ax[0];
+  Box* node_box = W.alloc<Box>(n);  // a node's bounds at its last position
+  const int nc = (n + kSegChunk - 1) / kSegChunk;
+  Seg<Box>* box_fwd = W.alloc<Seg<Box>>(3 * (size_t)nc);
+  Seg<Box>* box_bwd = W.alloc<Seg<Box>>(3 * (size_t)nc);
+  Seg<TypeCounts>* cnt_fwd = c.weighted ? W.alloc<Seg<TypeCounts>>(3 * (size_t)nc) : nullptr;
+  Seg<TypeCounts>* cnt_bwd = c.weighted ? W.alloc<Seg<TypeCounts>>(3 * (size_t)nc) : nullptr;
   WeightChains chains;
   for (int a = 0; a < 3; ++a) {
     chains.w[a] = W.alloc<double>(n);
@@ -960,8 +1166,6 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
     cost[a] = W.alloc<double>(n);
     bound[a] = c.weighted ? W.alloc<double>(n) : nullptr;
   }
-  TypeCounts* onehot = c.weighted ? W.alloc<TypeCounts>(n) : nullptr;
-  TypeCounts* cscan = c.weighted ? W.alloc<TypeCounts>(n) : nullptr;
   int* g_of_node = W.alloc<int>(cap);
   int* small_list = W.alloc<int>(cap);
   int* failed = W.alloc<int>(cap);
@@ -992,26 +1196,11 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
   int* counters = W.alloc<int>(8);  // node counter, next count, stats[4]
   int* root_start = W.alloc<int>(4);
   int* root_end = W.alloc<int>(4);
-  size_t tmp_bytes = 0, b1 = 0, b2 = 0, b3 = 0;
+  size_t tmp_bytes = 0, b1 = 0, b3 = 0, b4 = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, b1, skeys, skeys2, svals, svals, n);
-  cub::DeviceScan::InclusiveScanByKey(nullptr, b2, key, boxes, pre0, BoxUnion(), n);
-  {
-    size_t b2r = 0;
-    thrust::counting_iterator<int> count(0);
-    auto rkey = thrust::make_transform_iterator(count, ReverseKey{key, n});
-    auto rbox = thrust::make_transform_iterator(count, ReverseBox{boxes, n});
-    cub::DeviceScan::InclusiveScanByKey(nullptr, b2r, rkey, rbox, pre0, BoxUnion(), n);
-    b2 = std::max(b2, b2r);
-  }
   cub::DeviceScan::ExclusiveSum(nullptr, b3, flags, lscan, std::max(n, cap));
-  tmp_bytes = std::max(b1, std::max(b2, b3));
-  size_t b4 = 0, b5 = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, b4, tkeys, tkeys2, svals, svals, n, 0, 2);
-  tmp_bytes = std::max(tmp_bytes, b4);
-  if (c.weighted) {
-    cub::DeviceScan::InclusiveScanByKey(nullptr, b5, key, onehot, cscan, CountsAdd(), n);
-    tmp_bytes = std::max(tmp_bytes, b5);
-  }
+  tmp_bytes = std::max(b1, std::max(b3, b4));
   void* tmp = W.alloc<char>(tmp_bytes);
   if (!W.ok) return fail(ctx, RTB_ERR_OUT_OF_MEMORY, "BVH build workspace");
 
@@ -1065,11 +1254,20 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
   int sequential_nodes = 0;
   std::vector<int> level_begin = {0};
   int k = (int)h_big.size(), level = 0, total_nodes = roots;
+  const dim3 seg_grid(nc, 3), carry_grid(3, 2);
+  // split costs of every position on all three axes (and the level's node bounds)
   auto costs = [&](int certified) {
-    for (int a = 0; a < 3; ++a)
-      k_costs<<<blocks(n), 256, 0, sm>>>(P, I.a[a], N, key, level_of, level, a, n, pre_ax[a],
-                                         suf_ax[a], chains.pw[a], chains.sw[a], c.traversal,
-                                         certified, cost[a], bound[a]);
+    BoxLoad L;
+    L.P = P;
+    L.I = I;
+    L.level_of = level_of;
+    L.level = level;
+    SplitCosts U{P, I, N, {chains.pw[0], chains.pw[1], chains.pw[2]},
+                 {chains.sw[0], chains.sw[1], chains.sw[2]}, c.traversal, certified,
+                 {cost[0], cost[1], cost[2]}, {bound[0], bound[1], bound[2]}, node_box};
+    k_seg_chunks<<<seg_grid, kSegThreads, 0, sm>>>(L, key, n, nc, box_fwd, box_bwd);
+    k_seg_carries<BoxOp><<<carry_grid, kCarryThreads, 0, sm>>>(nc, box_fwd, box_bwd);
+    k_seg_apply<<<seg_grid, kSegThreads, 0, sm>>>(L, U, key, n, nc, box_fwd, box_bwd);
   };
   auto argmin = [&]() {
     k_arg_chunk_counts<<<blocks(k), 256, 0, sm>>>(N, active, k, arg_counts,
@@ -1095,29 +1293,20 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
       k_split_lists<<<blocks(k), 256, 0, sm>>>(N, active, k, small_list, lists, g_of_node);
       k_weights_seq<<<blocks(6LL * 32 * k, 128), 128, 0, sm>>>(chains, N, small_list, k, lists);
       if (certify) {
-        for (int a = 0; a < 3; ++a) {
-          k_type_onehot<<<blocks(n), 256, 0, sm>>>(P, I.a[a], n, onehot);
-          size_t tb = tmp_bytes;
-          cub::DeviceScan::InclusiveScanByKey(tmp, tb, key, onehot, cscan, CountsAdd(), n,
-                                              cub::Equality(), sm);
-          k_weights_counts<<<blocks(n), 256, 0, sm>>>(N, key, level_of, level, n, cscan, tw,
-                                                      chains.pw[a], chains.sw[a]);
-        }
+        CountLoad L;
+        L.P = P;
+        L.I = I;
+        L.N = N;
+        L.level_of = level_of;
+        L.level = level;
+        CountWeights U{tw, {chains.pw[0], chains.pw[1], chains.pw[2]},
+                       {chains.sw[0], chains.sw[1], chains.sw[2]}};
+        k_seg_chunks<<<seg_grid, kSegThreads, 0, sm>>>(L, key, n, nc, cnt_fwd, cnt_bwd);
+        k_seg_carries<CountOp><<<carry_grid, kCarryThreads, 0, sm>>>(nc, cnt_fwd, cnt_bwd);
+        k_seg_apply<<<seg_grid, kSegThreads, 0, sm>>>(L, U, key, n, nc, cnt_fwd, cnt_bwd);
       }
     } else {
       k_weights_unit<<<blocks(n), 256, 0, sm>>>(N, key, level_of, level, n, chains.pw[0], chains.sw[0]);
-    }
-    for (int a = 0; a < 3; ++a) {
-      size_t tb = tmp_bytes;
-      k_gather_boxes<<<blocks(n), 256, 0, sm>>>(P, I.a[a], n, boxes);
-      cub::DeviceScan::InclusiveScanByKey(tmp, tb, key, boxes, pre_ax[a], BoxUnion(), n,
-                                          cub::Equality(), sm);
-      tb = tmp_bytes;
-      thrust::counting_iterator<int> count(0);
-      auto rkey = thrust::make_transform_iterator(count, ReverseKey{key, n});
-      auto rbox = thrust::make_transform_iterator(count, ReverseBox{boxes, n});
-      cub::DeviceScan::InclusiveScanByKey(tmp, tb, rkey, rbox, suf_ax[a], BoxUnion(), n,
-                                          cub::Equality(), sm);
     }
     costs(certify ? 1 : 0);
     argmin();
@@ -1144,7 +1333,7 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
     }
     cudaMemsetAsync(counters + 1, 0, 4, sm);
     cudaMemsetAsync(counters + 6, 0, 4, sm);
-    k_decide<<<blocks(k), 256, 0, sm>>>(P, I, N, active, k, best_cost, best_flat, pre0, c.leaf_size,
+    k_decide<<<blocks(k), 256, 0, sm>>>(P, I, N, active, k, best_cost, best_flat, node_box, c.leaf_size,
                                         counters, next_active, counters + 1, level_of, level,
                                         counters + 2, counters + 6, sub_roots, counters + 7);
     k_sides<<<blocks(n), 256, 0, sm>>>(I, N, key, level_of, level, n, side);
