@@ -607,19 +607,20 @@ __global__ void k_argmin_flat(int blocks_total, const double* part_cost, const l
 // the deep levels.
 constexpr int kSubtreeSize = kSeqNodeSize;
 constexpr int kSubtreeThreads = 96;  // one warp per axis
+#ifndef RTB_SUBTREE_BLOCKS_PER_SM
+#define RTB_SUBTREE_BLOCKS_PER_SM 9  // 22.8 KB of shared memory and <= 72 registers each
+#endif
 
 struct SubtreeSmem {
   // The subtree's primitives get local slots 0..M-1 (axis 0's order at the root); the
-  // axis orders hold slots, and the primitives' boxes, weights and centroids are staged
-  // by slot, so the sweeps read shared memory only.
+  // axis orders hold slots, and the primitives' boxes and weights are staged by slot, so
+  // the sweeps read shared memory only.
   int gid[kSubtreeSize];        // slot -> primitive
   Box lbox[kSubtreeSize];
   double lw[kSubtreeSize];
-  double lcen[3][kSubtreeSize];
   unsigned char lside[kSubtreeSize];
   int idx[3][kSubtreeSize];     // the subtree's three axis orders (slots)
-  Box sbox[3][kSubtreeSize];    // per axis: suffix boxes of the current node
-  double sw[3][kSubtreeSize];   // per axis: suffix weights
+  double sterm[3][kSubtreeSize];  // per axis: suffix area x suffix weight of the current node
   int tmp[3][kSubtreeSize];     // per axis: partition scratch
   int stack[kSubtreeSize];      // pending nodes (depth first)
   double best_cost[3];
@@ -636,9 +637,10 @@ __device__ __forceinline__ Box empty_box() {
   return b;
 }
 
-// Inclusive union over lanes 0..lane (min / max are exact in any order).
-__device__ __forceinline__ Box warp_union_scan(Box b, int lane) {
-  for (int off = 1; off < 32; off <<= 1) {
+// Inclusive union over lanes 0..lane (min / max are exact in any order), for the lanes
+// below `count` (warp-uniform); lanes from `count` up hold empty boxes and are not needed.
+__device__ __forceinline__ Box warp_union_scan(Box b, int lane, int count) {
+  for (int off = 1; off < count; off <<= 1) {
     Box o;
     for (int k = 0; k < 3; ++k) {
       o.mn[k] = __shfl_up_sync(0xFFFFFFFFu, b.mn[k], off);
@@ -658,19 +660,22 @@ __device__ __forceinline__ Box warp_bcast(const Box& b, int src) {
   return r;
 }
 
-// Running sums of the 32 lanes' weights in lane order, continuing `acc`: lane q gets
-// acc + w_0 + ... + w_q added one by one.  Lanes past the node's end carry w = 0, and
-// adding +0 to a non-negative sum leaves it unchanged, so every chunk runs all 32 steps:
-// the 32 shuffles are issued ahead of the strictly sequential additions.
-__device__ __forceinline__ double warp_sequential_sum(double w, double& acc, int lane) {
-  double v[32];
-#pragma unroll
-  for (int q = 0; q < 32; ++q) v[q] = __shfl_sync(0xFFFFFFFFu, w, q);
+// Running sums of the lanes' weights in lane order, continuing `acc`: lane q gets
+// acc + w_0 + ... + w_q added one by one, for the lanes below `count` (warp-uniform).  The
+// chain runs in groups of four lanes, each group's shuffles issued ahead of its additions;
+// lanes past the node's end carry w = 0, and adding +0 to a non-negative sum leaves it
+// unchanged, so the last group may run past `count`.
+__device__ __forceinline__ double warp_sequential_sum(double w, double& acc, int lane, int count) {
   double mine = 0.0;
+  for (int g = 0; g < count; g += 4) {
+    double v[4];
 #pragma unroll
-  for (int q = 0; q < 32; ++q) {
-    acc = acc + v[q];
-    mine = q == lane ? acc : mine;
+    for (int q = 0; q < 4; ++q) v[q] = __shfl_sync(0xFFFFFFFFu, w, g + q);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      acc = acc + v[q];
+      mine = g + q == lane ? acc : mine;
+    }
   }
   return mine;
 }
@@ -683,7 +688,7 @@ __device__ __forceinline__ bool lex_less(double c, long long f, double bc, long 
 // the block takes the first minimum over the three axes' winners, and the warps of the two
 // other axes partition their orders.  Every decision is computed identically by all threads
 // (or broadcast through shared memory), so the block's barriers are uniform.
-__global__ void __launch_bounds__(kSubtreeThreads) k_subtrees(
+__global__ void __launch_bounds__(kSubtreeThreads, RTB_SUBTREE_BLOCKS_PER_SM) k_subtrees(
     const Prims P, IdxSet I, Nodes N, const int* roots, const int* root_count, int leaf_size,
     double traversal, int* node_counter, int* stats, int* slot_of) {
   __shared__ SubtreeSmem sm;
@@ -696,7 +701,6 @@ __global__ void __launch_bounds__(kSubtreeThreads) k_subtrees(
     sm.gid[i] = p;
     sm.lbox[i] = P.box[p];
     sm.lw[i] = P.w[p];
-    for (int a = 0; a < 3; ++a) sm.lcen[a][i] = P.cen[a][p];
     slot_of[p] = i;  // each primitive belongs to one subtree
     sm.idx[0][i] = i;
   }
@@ -734,36 +738,35 @@ __global__ void __launch_bounds__(kSubtreeThreads) k_subtrees(
     long long best_flat = 0x7FFFFFFFFFFFFFFFLL;
     const int a = warp;
     const int* ix = sm.idx[a] + lo;
-    if (m > 1 && sm.lcen[a][ix[m - 1]] - sm.lcen[a][ix[0]] > 1.0e-12) {
+    if (m > 1 && P.cen[a][sm.gid[ix[m - 1]]] - P.cen[a][sm.gid[ix[0]]] > 1.0e-12) {
       // suffix boxes and weights, from the last position down (GpuScene.java:1476-1480)
       Box carry = empty_box();
       double acc = 0.0;
       for (int base = 0; base < m; base += 32) {
+        const int cnt = min(32, m - base);
         int q = m - 1 - (base + lane);
         Box b = q >= 0 ? sm.lbox[ix[q]] : empty_box();
         double w = q >= 0 ? sm.lw[ix[q]] : 0.0;
-        b = BoxUnion()(warp_union_scan(b, lane), carry);
-        double sw = warp_sequential_sum(w, acc, lane);
-        if (q >= 0) {
-          sm.sbox[a][lo + q] = b;
-          sm.sw[a][lo + q] = sw;
-        }
-        carry = warp_bcast(b, 31);
+        b = BoxUnion()(warp_union_scan(b, lane, cnt), carry);
+        double sw = warp_sequential_sum(w, acc, lane, cnt);
+        if (q >= 0) sm.sterm[a][lo + q] = surface_area(b) * sw;
+        carry = warp_bcast(b, cnt - 1);
       }
       __syncwarp();
       // prefix pass and the cost of putting local positions [0, i) left (1470-1475, 1482-1485)
       carry = empty_box();
       acc = 0.0;
       for (int base = 0; base < m; base += 32) {
+        const int cnt = min(32, m - base);
         int li = base + lane;
         Box b = li < m ? sm.lbox[ix[li]] : empty_box();
         double w = li < m ? sm.lw[ix[li]] : 0.0;
-        b = BoxUnion()(warp_union_scan(b, lane), carry);
-        double pw = warp_sequential_sum(w, acc, lane);
+        b = BoxUnion()(warp_union_scan(b, lane, cnt), carry);
+        double pw = warp_sequential_sum(w, acc, lane, cnt);
         int i = li + 1;  // split after li
         if (i < m) {
           double bl = surface_area(b) * pw;
-          double d = surface_area(sm.sbox[a][lo + i]) * sm.sw[a][lo + i];
+          double d = sm.sterm[a][lo + i];
           double c = (node_a + bl) + d;
           long long flat = (long long)a * m + i;
           if (lex_less(c, flat, best, best_flat)) {
@@ -771,7 +774,7 @@ __global__ void __launch_bounds__(kSubtreeThreads) k_subtrees(
             best_flat = flat;
           }
         }
-        carry = warp_bcast(b, 31);
+        carry = warp_bcast(b, cnt - 1);
       }
       for (int off = 16; off > 0; off >>= 1) {
         double oc = __shfl_xor_sync(0xFFFFFFFFu, best, off);
