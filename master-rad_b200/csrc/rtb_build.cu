@@ -171,7 +171,10 @@ struct TypeWeights {
 // position of a node at the current level do no work (a node at the level never spans
 // such a chunk).  Box unions (min / max) and integer sums are exact, so any association of
 // them gives the sequential result bit for bit.
-constexpr int kSegThreads = 256, kSegItems = 4, kSegChunk = kSegThreads * kSegItems;
+#ifndef RTB_SEG_ITEMS
+#define RTB_SEG_ITEMS 4
+#endif
+constexpr int kSegThreads = 256, kSegItems = RTB_SEG_ITEMS, kSegChunk = kSegThreads * kSegItems;
 constexpr int kSegWarps = kSegThreads / 32, kCarryThreads = 1024;
 
 template <class V>
