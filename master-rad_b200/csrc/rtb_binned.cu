@@ -622,7 +622,7 @@ rtb_status build_bvh_binned(rtb_context* ctx, const rtb_scene_desc* desc, const 
   cudaMemsetAsync(N.order_axis, 0, (size_t)roots * 4, sm);
   cudaMemsetAsync(N.depth, 0, (size_t)roots * 4, sm);
   cudaMemsetAsync(level_of, 0, (size_t)roots * 4, sm);
-  k_init_keys<<<roots, 256, 0, sm>>>(key, root_start, root_end, roots);
+  k_init_keys<<<blocks(n), 256, 0, sm>>>(key, root_start, root_end, roots, n);
 
   SplitCfg S;
   S.bins = bins;

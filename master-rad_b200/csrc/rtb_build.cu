@@ -455,14 +455,10 @@ struct SplitCosts {
   }
 };
 
-// Nodes of this level split into those summed sequentially (small) and those certified.
-__global__ void k_split_lists(const Nodes N, const int* active, int k, int* small, int* small_count,
-                              int* g_of_node) {
+// Each active node's slot in the level's per-node arrays.
+__global__ void k_node_slots(const int* active, int k, int* g_of_node) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= k) return;
-  int node = active[g];
-  g_of_node[node] = g;
-  if (N.end[node] - N.start[node] <= kSeqNodeSize) small[atomicAdd(small_count, 1)] = node;
+  if (g < k) g_of_node[active[g]] = g;
 }
 
 // The winner's bound, and a cleared failure flag, per certified node.
@@ -483,12 +479,16 @@ __global__ void k_best_bound(const Nodes N, const int* active, int k, const doub
 
 // A certified node fails when some other candidate could, in the reference's rounding, cost
 // as little as the winner.
-__global__ void k_certify(const Nodes N, const int* key, const int* level_of, int level, int axis,
-                          int n, const int* g_of_node, const double* cost, const double* bound,
-                          const double* best_cost, const long long* best_flat,
+__global__ void k_certify(const Nodes N, const int* key, const int* level_of, int level, int n,
+                          const int* g_of_node, const double* cost0, const double* cost1,
+                          const double* cost2, const double* bound0, const double* bound1,
+                          const double* bound2, const double* best_cost, const long long* best_flat,
                           const double* best_bound, int* failed) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
+  const int axis = blockIdx.y;  // one axis per grid row
+  const double* cost = axis == 0 ? cost0 : axis == 1 ? cost1 : cost2;
+  const double* bound = axis == 0 ? bound0 : axis == 1 ? bound1 : bound2;
   int node = key[j];
   if (level_of[node] != level) return;
   int s = N.start[node], len = N.end[node] - s;
@@ -882,15 +882,52 @@ __global__ void __launch_bounds__(kSubtreeThreads, RTB_SUBTREE_BLOCKS_PER_SM) k_
   }
 }
 
-// Nodes per depth, then all nodes listed level by level (the finishing passes walk them).
-__global__ void k_depth_hist(const Nodes N, int count, int* hist) {
-  int node = blockIdx.x * blockDim.x + threadIdx.x;
-  if (node < count) atomicAdd(hist + N.depth[node], 1);
+// Nodes per depth, then all nodes listed level by level (the finishing passes walk them;
+// the order inside a level is free, every node of a level being independent of the
+// others).  Both passes count in shared memory first, a warp's lanes of equal depth
+// together, so that each block adds once per depth to the few global counters instead of
+// once per node; depths from kDepthShared up go to the global counters directly.
+constexpr int kDepthShared = 256;
+
+__global__ void __launch_bounds__(256) k_depth_hist(const Nodes N, int count, int* hist) {
+  __shared__ int sh[kDepthShared];
+  for (int i = threadIdx.x; i < kDepthShared; i += blockDim.x) sh[i] = 0;
+  __syncthreads();
+  const int node = blockIdx.x * blockDim.x + threadIdx.x;
+  const int d = node < count ? N.depth[node] : -1;
+  const unsigned peers = __match_any_sync(0xFFFFFFFFu, d);
+  if (d >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) {
+    if (d < kDepthShared) atomicAdd(sh + d, __popc(peers));
+    else atomicAdd(hist + d, __popc(peers));
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kDepthShared; i += blockDim.x)
+    if (sh[i]) atomicAdd(hist + i, sh[i]);
 }
 
-__global__ void k_depth_scatter(const Nodes N, int count, int* cursor, int* all_nodes) {
-  int node = blockIdx.x * blockDim.x + threadIdx.x;
-  if (node < count) all_nodes[atomicAdd(cursor + N.depth[node], 1)] = node;
+__global__ void __launch_bounds__(256) k_depth_scatter(const Nodes N, int count, int* cursor,
+                                                       int* all_nodes) {
+  __shared__ int cnt[kDepthShared], base[kDepthShared];
+  for (int i = threadIdx.x; i < kDepthShared; i += blockDim.x) cnt[i] = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int node = blockIdx.x * blockDim.x + threadIdx.x;
+  const int d = node < count ? N.depth[node] : -1;
+  const unsigned peers = __match_any_sync(0xFFFFFFFFu, d);
+  const int leader = __ffs(peers) - 1;
+  int local = -1;  // rank among the block's nodes of depth d
+  if (d >= 0 && d < kDepthShared) {
+    int first = 0;
+    if (lane == leader) first = atomicAdd(cnt + d, __popc(peers));
+    local = first;
+  }
+  local = __shfl_sync(0xFFFFFFFFu, local, leader) + __popc(peers & ((1u << lane) - 1u));
+  __syncthreads();
+  for (int i = threadIdx.x; i < kDepthShared; i += blockDim.x)
+    if (cnt[i]) base[i] = atomicAdd(cursor + i, cnt[i]);
+  __syncthreads();
+  if (d >= kDepthShared) all_nodes[atomicAdd(cursor + d, 1)] = node;
+  else if (d >= 0) all_nodes[base[d] + local] = node;
 }
 
 // Leaf-or-split decision per active node (GpuScene.java:1424-1447).
@@ -953,6 +990,37 @@ __global__ void k_decide(const Prims P, IdxSet I, Nodes N, const int* active, in
       atomicMax(largest_child, sizes[h]);
     }
   }
+}
+
+// Stable partition of the three axis orders of every node split at this level, one axis
+// per blockIdx.y: left flags, one exclusive sum over all 3n flags (a node's left rank is a
+// difference inside its own axis range, so the other axes' counts cancel), then the scatter.
+__global__ void k_left_flags3(IdxSet I, const Nodes N, const int* key, const int* level_of, int level,
+                              int n, const unsigned char* side, int* flags) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int a = blockIdx.y;
+  const int node = key[j];
+  const bool split = level_of[node] == level && N.split_axis[node] >= 0;
+  flags[(size_t)a * n + j] = split ? (side[I.a[a][j]] == 0) : 0;
+}
+
+__global__ void k_scatter3(IdxSet I, IdxSet T, const Nodes N, const int* key, const int* level_of,
+                           int level, int n, const unsigned char* side, const int* lscan) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int a = blockIdx.y;
+  const int node = key[j];
+  const int p = I.a[a][j];
+  int* out = T.a[a];
+  if (!(level_of[node] == level && N.split_axis[node] >= 0)) {
+    out[j] = p;
+    return;
+  }
+  const int* ls = lscan + (size_t)a * n;
+  const int s = N.start[node];
+  const int lrank = ls[j] - ls[s];
+  out[side[p] == 0 ? s + lrank : s + N.split_pos[node] + ((j - s) - lrank)] = p;
 }
 
 __global__ void k_sides(IdxSet I, const Nodes N, const int* key, const int* level_of, int level, int n,
@@ -1173,7 +1241,6 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
     bound[a] = c.weighted ? W.alloc<double>(n) : nullptr;
   }
   int* g_of_node = W.alloc<int>(cap);
-  int* small_list = W.alloc<int>(cap);
   int* failed = W.alloc<int>(cap);
   int* failed_list = W.alloc<int>(cap);
   double* best_bound = W.alloc<double>(cap);
@@ -1181,8 +1248,8 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
   int* sub_roots = W.alloc<int>(cap);  // nodes whose subtrees k_subtrees builds
   int* depth_hist = W.alloc<int>(cap + 1);
   unsigned char* side = W.alloc<unsigned char>(n);
-  int* flags = W.alloc<int>(n);
-  int* lscan = W.alloc<int>(n);
+  int* flags = W.alloc<int>(3 * (size_t)n);  // left flags of the three axis orders
+  int* lscan = W.alloc<int>(3 * (size_t)n);
   unsigned long long* skeys = W.alloc<unsigned long long>(n);
   unsigned long long* skeys2 = W.alloc<unsigned long long>(n);
   int* svals = W.alloc<int>(n);
@@ -1204,7 +1271,7 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
   int* root_end = W.alloc<int>(4);
   size_t tmp_bytes = 0, b1 = 0, b3 = 0, b4 = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, b1, skeys, skeys2, svals, svals, n);
-  cub::DeviceScan::ExclusiveSum(nullptr, b3, flags, lscan, std::max(n, cap));
+  cub::DeviceScan::ExclusiveSum(nullptr, b3, flags, lscan, std::max(3 * n, cap));
   cub::DeviceRadixSort::SortPairs(nullptr, b4, tkeys, tkeys2, svals, svals, n, 0, 2);
   tmp_bytes = std::max(b1, std::max(b3, b4));
   void* tmp = W.alloc<char>(tmp_bytes);
@@ -1250,13 +1317,11 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
   cudaMemsetAsync(N.order_axis, 0xFF, (size_t)roots * 4, sm);  // -1: input order
   cudaMemsetAsync(N.depth, 0, (size_t)roots * 4, sm);
   cudaMemcpyAsync(level_of, h_level.data(), roots * 4, cudaMemcpyHostToDevice, sm);
-  k_init_keys<<<roots, 256, 0, sm>>>(key, root_start, root_end, roots);
+  k_init_keys<<<blocks(n), 256, 0, sm>>>(key, root_start, root_end, roots, n);
 
   // ---- level loop
   TypeWeights tw;
   for (int t = 0; t < 4; ++t) tw.w[t] = c.weighted ? 1.0 + c.lambda * (c.measured[t] - 1.0) : 1.0;
-  int largest = 0;  // primitives in the level's largest node
-  for (int r : h_big) largest = std::max(largest, h_re[r] - h_rs[r]);
   int sequential_nodes = 0;
   std::vector<int> level_begin = {0};
   int k = (int)h_big.size(), level = 0, total_nodes = roots;
@@ -1289,16 +1354,16 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
                                               best_flat);
   };
   while (k > 0) {
-    const bool certify = c.weighted && largest > kSeqNodeSize;
-    // weight sums of all three axis orders first: sequential chains for the small nodes (one
-    // launch), per-type counts for the large ones
+    // Every node of the level loop holds more than kSubtreeSize >= kSeqNodeSize primitives
+    // (smaller ones go to k_subtrees), so with non-unit weights all of them take the
+    // certified count-based weights; only those whose certificate fails are summed
+    // sequentially, below.
+    static_assert(kSubtreeSize >= kSeqNodeSize, "level-loop nodes must all be certifiable");
+    const bool certify = c.weighted;
     if (c.weighted) {
-      for (int a = 0; a < 3; ++a)
-        k_gather_weights<<<blocks(n), 256, 0, sm>>>(P, I.a[a], n, const_cast<double*>(chains.w[a]));
       cudaMemsetAsync(lists, 0, 2 * sizeof(int), sm);
-      k_split_lists<<<blocks(k), 256, 0, sm>>>(N, active, k, small_list, lists, g_of_node);
-      k_weights_seq<<<blocks(6LL * 32 * k, 128), 128, 0, sm>>>(chains, N, small_list, k, lists);
-      if (certify) {
+      k_node_slots<<<blocks(k), 256, 0, sm>>>(active, k, g_of_node);
+      {
         CountLoad L;
         L.P = P;
         L.I = I;
@@ -1321,15 +1386,17 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
       // their costs again, and the argmin again (unchanged for every other node)
       k_best_bound<<<blocks(k), 256, 0, sm>>>(N, active, k, best_cost, best_flat, bound[0], bound[1],
                                               bound[2], best_bound, failed);
-      for (int a = 0; a < 3; ++a)
-        k_certify<<<blocks(n), 256, 0, sm>>>(N, key, level_of, level, a, n, g_of_node, cost[a],
-                                             bound[a], best_cost, best_flat, best_bound, failed);
+      k_certify<<<dim3(blocks(n), 3), 256, 0, sm>>>(N, key, level_of, level, n, g_of_node, cost[0],
+                                                    cost[1], cost[2], bound[0], bound[1], bound[2],
+                                                    best_cost, best_flat, best_bound, failed);
       k_failed_list<<<blocks(k), 256, 0, sm>>>(active, k, failed, failed_list, lists + 1);
       int nfail = 0;
       cudaMemcpyAsync(&nfail, lists + 1, 4, cudaMemcpyDeviceToHost, sm);
       cudaError_t e = cudaStreamSynchronize(sm);
       if (e != cudaSuccess) return cuda_fail(ctx, e, "BVH build level");
       if (nfail > 0) {
+        for (int a = 0; a < 3; ++a)
+          k_gather_weights<<<blocks(n), 256, 0, sm>>>(P, I.a[a], n, const_cast<double*>(chains.w[a]));
         k_weights_seq<<<blocks(6LL * 32 * nfail, 128), 128, 0, sm>>>(chains, N, failed_list, nfail,
                                                                      nullptr);
         costs(0);
@@ -1343,12 +1410,13 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
                                         counters, next_active, counters + 1, level_of, level,
                                         counters + 2, counters + 6, sub_roots, counters + 7);
     k_sides<<<blocks(n), 256, 0, sm>>>(I, N, key, level_of, level, n, side);
-    for (int a = 0; a < 3; ++a) {
-      k_left_flags<<<blocks(n), 256, 0, sm>>>(I.a[a], N, key, level_of, level, n, side, flags);
+    {
+      const dim3 axes_grid(blocks(n), 3);
+      k_left_flags3<<<axes_grid, 256, 0, sm>>>(I, N, key, level_of, level, n, side, flags);
       size_t tb = tmp_bytes;
-      cub::DeviceScan::ExclusiveSum(tmp, tb, flags, lscan, n, sm);
-      k_scatter<<<blocks(n), 256, 0, sm>>>(I.a[a], N, key, level_of, level, n, side, lscan, T.a[a]);
-      std::swap(I.a[a], T.a[a]);
+      cub::DeviceScan::ExclusiveSum(tmp, tb, flags, lscan, 3 * n, sm);
+      k_scatter3<<<axes_grid, 256, 0, sm>>>(I, T, N, key, level_of, level, n, side, lscan);
+      for (int a = 0; a < 3; ++a) std::swap(I.a[a], T.a[a]);
     }
     k_update_keys<<<blocks(n), 256, 0, sm>>>(N, level_of, level, n, key);
     int next_info[6] = {0, 0, 0, 0, 0, 0};  // counters[1..6]: next count, ..., largest child
@@ -1356,7 +1424,6 @@ rtb_status build_bvh_options(rtb_context* ctx, const rtb_scene_desc* desc, const
     cudaError_t e = cudaStreamSynchronize(sm);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "BVH build level");
     int next = next_info[0];
-    largest = next_info[5];
     if (next > 0) std::swap(active, next_active);
     k = next;
     level++;

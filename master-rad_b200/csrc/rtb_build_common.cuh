@@ -140,9 +140,12 @@ struct Nodes {
   double* sah[3];   // generalized, uniform, weighted
 };
 
-__global__ void k_init_keys(int* key, const int* start, const int* end, int roots) {
-  int r = blockIdx.x;
-  for (int j = start[r] + threadIdx.x; j < end[r]; j += blockDim.x) key[j] = r;
+// key[j] = the root whose range [start, end) holds position j (at most four roots).
+__global__ void k_init_keys(int* key, const int* start, const int* end, int roots, int n) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  for (int r = 0; r < roots; ++r)
+    if (j >= start[r] && j < end[r]) key[j] = r;
 }
 
 __device__ __forceinline__ int current_prim(const int* const* idx, int order_axis, int j) {
