@@ -55,16 +55,21 @@ from rtb200.tracer import Context, ResidentScene, build_config, camera_struct, s
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 # dram__bytes_read.sum + dram__bytes_write.sum of k_render per sample, from one ncu capture
-# of the same scene at 1024x768x4 spp (profiles/k_render_hetero10k_1024x768x4spp_full.md);
-# workloads without a capture report null traffic.
-TRAFFIC_BYTES_PER_SAMPLE = {"hetero": (26.58e6 + 143.07e6) / 3145728}
-# smsp__inst_executed.sum of k_render per sample from the same capture (8.862 G warp
-# instructions for 3,145,728 samples), for the issue bound: warp instructions per second
-# against one instruction per cycle on each of the 4 schedulers of every SM.
-INST_PER_SAMPLE = {"hetero": 8.862e9 / 3145728}
-# smsp__thread_inst_executed_per_inst_executed of the same capture: active lanes per warp
+# of the same scene at a smaller frame: the 10k scene at 1024x768x4 spp
+# (profiles/k_render_hetero10k_1024x768x4spp_full.md), the 1M scene at 480x270x4 spp
+# (profiles/k_render_scale1M_480x270x4spp_full.md); workloads without a capture report
+# null traffic.
+CAPTURE_FRAME = {"hetero": "1024x768x4spp", "scale": "480x270x4spp"}
+TRAFFIC_BYTES_PER_SAMPLE = {"hetero": (26.58e6 + 143.07e6) / 3145728,
+                            "scale": (359.48e6 + 153.86e6) / 518400}
+# smsp__inst_executed.sum of k_render per sample from the same captures (8.862 G warp
+# instructions for 3,145,728 samples; 2.823 G for 518,400), for the issue bound: warp
+# instructions per second against one instruction per cycle on each of the 4 schedulers of
+# every SM.
+INST_PER_SAMPLE = {"hetero": 8.862e9 / 3145728, "scale": 2.8227e9 / 518400}
+# smsp__thread_inst_executed_per_inst_executed of the same captures: active lanes per warp
 # instruction, which scales the issue bound to lane-instructions doing useful work.
-LANES_PER_INST = {"hetero": 9.22}
+LANES_PER_INST = {"hetero": 9.22, "scale": 9.48}
 
 
 def issue_roofline(workload, samples, launch_ms, sm_count, sm_mhz):
@@ -78,8 +83,8 @@ def issue_roofline(workload, samples, launch_ms, sm_count, sm_mhz):
     return {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "warp-inst/s",
             "frac": achieved / peak, "inst_per_launch": inst,
             "active_lanes_per_inst": lanes, "useful_lane_frac": achieved / peak * lanes / 32.0,
-            "note": "instructions per sample from the ncu capture of a 1024x768x4spp frame of "
-                    "the same scene, scaled by samples; peak = SMs x 4 schedulers x the SM "
+            "note": "instructions per sample from the ncu capture of a " + CAPTURE_FRAME[workload] +
+                    " frame of the same scene, scaled by samples; peak = SMs x 4 schedulers x the SM "
                     "clock sampled during the timed frames; useful_lane_frac also counts the "
                     "lanes a warp instruction leaves idle (divergent paths)"}
 
@@ -441,10 +446,12 @@ def run_batched(args, rank=0, world=1, local=0):
     finish_ranks(world)
 
 
-def frames_measure(ctx, w, steps, warmup, flush, stream, ref_frames=0):
+def frames_measure(ctx, w, steps, warmup, flush, stream, ref_frames=0, sm_mhz=None):
     """Device build and frames of one configuration on one GPU: median build ms, Msamples/s
     over `steps` frames (CUDA events around each frame, L2 flushed before each outside the
-    events), and optionally the reference kernel on the same frame (ref_kernel_leg)."""
+    events), optionally the reference kernel on the same frame (ref_kernel_leg), and the
+    issue bound and traffic where this workload has an ncu capture (sm_mhz: the SM clock
+    sampled during the headline's timed frames)."""
     import torch
     builds = []
     for i in range(2):
@@ -475,6 +482,15 @@ def frames_measure(ctx, w, steps, warmup, flush, stream, ref_frames=0):
          "ms_per_frame": statistics.mean(ms), "frames": steps, "build_ms": builds[-1],
          "primitives": w.scene.bounded_primitive_count(),
          "frame": "%dx%d %dspp depth%d" % (w.width, w.height, w.spp, w.max_depth)}
+    if w.name in INST_PER_SAMPLE:
+        d["roofline_issue"] = issue_roofline(w.name, samples, statistics.mean(ms),
+                                             ctx.device_info().sm_count, sm_mhz)
+        d["traffic"] = {"bytes_per_frame": TRAFFIC_BYTES_PER_SAMPLE[w.name] * samples,
+                        "gbs": TRAFFIC_BYTES_PER_SAMPLE[w.name] * samples
+                               / (statistics.mean(ms) / 1e3) / 1e9,
+                        "note": "dram bytes per sample of the ncu capture of a %s frame of the "
+                                "same scene (cold caches), scaled by samples"
+                                % CAPTURE_FRAME[w.name]}
     if ref_frames:
         rk = ref_kernel_leg(w, _Tree(res.download_bvh()), ref_frames, flush.numel() * 4)
         if rk is not None:
@@ -485,7 +501,7 @@ def frames_measure(ctx, w, steps, warmup, flush, stream, ref_frames=0):
     return d
 
 
-def other_configs(ctx, local, flush):
+def other_configs(ctx, local, flush, sm_mhz=None):
     """The benchmark's other configurations, measured once after the headline timing so that
     one default run shows them all: the plain 64-sphere frame (with the reference kernel
     beside it), the 1M-primitive scene (device build and frames), the 64-scene batch with
@@ -495,7 +511,8 @@ def other_configs(ctx, local, flush):
     stream = torch.cuda.Stream(device=local)
     out = {}
     out["C1_plain"] = frames_measure(ctx, synth.plain_workload(), 10, 3, flush, stream, ref_frames=3)
-    out["C3_scale"] = frames_measure(ctx, synth.scale_workload(), 2, 1, flush, stream)
+    out["C3_scale"] = frames_measure(ctx, synth.scale_workload(), 2, 1, flush, stream,
+                                     sm_mhz=sm_mhz)
     works = synth.batched_workloads()
     m = batched_measure(ctx, local, works, 1, 1, autotune=False)
     samples = sum(w.width * w.height * w.spp for w in works)
@@ -879,8 +896,8 @@ def main():
                          "frac": achieved / peak,
                          "traffic": (TRAFFIC_BYTES_PER_SAMPLE[args.workload] * samples_per_frame
                                      if args.workload in TRAFFIC_BYTES_PER_SAMPLE else None),
-                         "traffic_note": ("ncu capture of a 1024x768x4spp frame of the same "
-                                          "scene, scaled by samples"
+                         "traffic_note": ("ncu capture of a %s frame of the same scene, scaled "
+                                          "by samples" % CAPTURE_FRAME.get(args.workload)
                                           if args.workload in TRAFFIC_BYTES_PER_SAMPLE
                                           else "no capture of this workload"),
                          "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
@@ -902,7 +919,8 @@ def main():
         if cpu is not None:
             line["cpu_baseline"] = cpu
         if world == 1 and args.workload == "hetero" and not args.no_other_configs:
-            line["other_configs"] = other_configs(ctx, local, flush)
+            line["other_configs"] = other_configs(
+                ctx, local, flush, clock_info.get("sm_mhz") or clock_info.get("sm_max_mhz"))
         if world == 1 and not args.no_ref_kernel:
             frames = args.ref_frames or (1 if args.workload == "scale" else 3)
             rk = ref_kernel_leg(w, _Tree(res.download_bvh()), frames, flush.numel() * 4)
