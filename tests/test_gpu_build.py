@@ -145,6 +145,17 @@ def test_device_build_one_million_identical(ctx):
     assert st.sequential_nodes <= st.node_count // 100
 
 
+@pytest.mark.slow
+def test_device_build_identical_beyond_one_tile_of_chunks(ctx):
+    """1.2M primitives: more than 1,024 scan chunks of 1,024 positions, so the segmented
+    scans carry their chunk aggregates across two tiles of the carry kernel (the root node
+    of the first level spans every chunk of both tiles)."""
+    w = synth.scale_workload(n=1_200_000)
+    st = _check_identical(ctx, w.scene, w.scene.config)
+    assert st.primitive_ref_count == 1_200_001
+    assert (st.primitive_ref_count + 1023) // 1024 > 1024
+
+
 @pytest.mark.parametrize("mode", [BvhBuildMode.SAH_ROTATIONS, BvhBuildMode.WEIGHTED_SAH_ROTATIONS])
 @pytest.mark.parametrize("n", [7, 300, 5000])
 def test_device_rotation_modes_identical(ctx, mode, n):
