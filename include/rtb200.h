@@ -36,7 +36,7 @@ typedef enum {
   RTB_ERR_UNAVAILABLE = 2,      /* no usable device (GpuRayTracer.isAvailable() false) */
   RTB_ERR_CUDA = 3,             /* a CUDA runtime call failed; see rtb_last_error */
   RTB_ERR_OUT_OF_MEMORY = 4,
-  RTB_ERR_UNSUPPORTED = 5,      /* a build mode this library does not implement */
+  RTB_ERR_UNSUPPORTED = 5,      /* a mode this library does not implement */
   RTB_ERR_DEVICE_CHECK = 6,     /* a kernel's own bounds / input check failed */
   RTB_ERR_WATCHDOG = 7,         /* a kernel gave up at its work budget or was aborted
                                    (IllegalStateException in GpuRayTracer.java:572-580) */
@@ -204,6 +204,18 @@ RTB_API rtb_status rtb_render_sample(rtb_context* ctx, rtb_scene* scene, const r
  * for the context's stream); returns after the launch is queued. */
 RTB_API rtb_status rtb_render_device(rtb_context* ctx, rtb_scene* scene, const rtb_camera* camera,
                              const rtb_render_params* params, float* rgb_device, void* stream);
+
+/* The same frame as rtb_render_device, bit for bit, computed in the wavefront form: one
+ * wave per sample index over all pixels; per bounce, one kernel traces every live path of
+ * the wave and one shades them (path state in device memory, held by the context and grown
+ * to the largest frame).  The A/B counterpart of the persistent kernel behind
+ * rtb_render_device, which is faster on the B200; no metrics build (RTB_ERR_UNSUPPORTED).
+ * No counterpart in the reference, whose renderKernel is one thread per pixel
+ * (GpuKernelSources.java:1167-1315). */
+RTB_API rtb_status rtb_render_device_wavefront(rtb_context* ctx, rtb_scene* scene,
+                                               const rtb_camera* camera,
+                                               const rtb_render_params* params,
+                                               float* rgb_device, void* stream);
 
 /* One frame's rows first_row, first_row + row_stride, ... (< height), packed densely into
  * rgb_device (3 floats per pixel, row k of the output = frame row first_row + k*row_stride).

@@ -162,6 +162,7 @@ rtb_status rtb_context_destroy(rtb_context* ctx) {
     cudaFree(ctx->d_abort);
     cudaFree(ctx->d_stage);
     cudaFree(ctx->d_tail);
+    cudaFree(ctx->d_wave);
     cudaFreeHost(ctx->h_pinned);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -330,6 +331,19 @@ rtb_status rtb_render_device(rtb_context* ctx, rtb_scene* scene, const rtb_camer
   ctx_acquire(ctx, sm);
   arm_abort(ctx, sm);
   rtb_status s = render_frame(ctx, scene, camera, params, rgb_device, sm, false);
+  ctx_release(ctx, sm);
+  return s;
+}
+
+rtb_status rtb_render_device_wavefront(rtb_context* ctx, rtb_scene* scene, const rtb_camera* camera,
+                                       const rtb_render_params* params, float* rgb_device,
+                                       void* stream) {
+  if (!ctx) return RTB_ERR_INVALID_ARGUMENT;
+  Guard g(ctx);
+  cudaStream_t sm = stream ? (cudaStream_t)stream : ctx->stream;
+  ctx_acquire(ctx, sm);
+  arm_abort(ctx, sm);
+  rtb_status s = render_frame_wavefront(ctx, scene, camera, params, rgb_device, sm);
   ctx_release(ctx, sm);
   return s;
 }

@@ -41,6 +41,9 @@ struct rtb_context {
   // Per-sample radiance of the frame's last pixels (rendered one sample per lane).
   float* d_tail = nullptr;
   size_t tail_bytes = 0;
+  // Path state of the wavefront form, grown to the largest frame rendered in that form.
+  void* d_wave = nullptr;
+  size_t wave_bytes = 0;
   int render_launches = 0;  // kernels the last render_frame launched
 };
 
@@ -98,6 +101,9 @@ void scene_free(rtb_scene* s, cudaStream_t stream);
 rtb_status render_frame(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
                         const rtb_render_params* p, float* d_rgb, cudaStream_t stream,
                         bool timed, int row0 = 0, int row_stride = 1);
+// The same frame in the wavefront form (whole frames, no metrics build).
+rtb_status render_frame_wavefront(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
+                                  const rtb_render_params* p, float* d_rgb, cudaStream_t stream);
 // One frame's launch, planned apart from where it runs (the batch's frames mode launches
 // many into one graph).  plan_frame validates and sizes; bind_frame gives it a queue head
 // (zeroed before launch), a sample buffer of frame_tail_bytes (nullptr: no single-sample

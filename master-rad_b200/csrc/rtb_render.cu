@@ -63,6 +63,76 @@ __device__ __forceinline__ uint32_t pixel_base_seed(unsigned long long frame_see
   return hash_u32(s);
 }
 
+// One path segment after its closest-hit query (tracePath loop body, K:1098-1162): the
+// background on a miss; else the hit's emission, the lobe chosen by luminance, and the
+// next ray with its throughput.  Returns true when the path ends.  Both frame forms (the
+// persistent k_render and the wavefront kernels) shade through this one function.
+__device__ __forceinline__ bool shade_segment(const DevScene& S, bool hit, const Best& b, float3& o,
+                                              float3& d, float3& thr, float3& rad, uint32_t& rng,
+                                              int& depth, int max_depth) {
+  if (!hit) {
+    rad = add(rad, mulv(thr, S.background));
+    return true;
+  }
+  float3 pos, n;
+  int mi;
+  hit_record(S, b, o, d, &pos, &n, &mi);
+  float4 m0 = make_float4(0, 0, 0, 0), m1 = m0, m2 = m0, m3 = m0;
+  if (mi >= 0) {
+    const float4* mp = S.materials + 4 * mi;
+    m0 = __ldg(mp);
+    m1 = __ldg(mp + 1);
+    m2 = __ldg(mp + 2);
+    m3 = __ldg(mp + 3);
+  }
+  float3 cd = v3(m0.x, m0.y, m0.z), cr = v3(m1.x, m1.y, m1.z), ct = v3(m2.x, m2.y, m2.z);
+  rad = add(rad, mulv(thr, v3(m3.x, m3.y, m3.z)));
+  float3 inc = neg(d);
+  float wd = luminance(cd), wr = luminance(cr), wt = luminance(ct);
+  float sum = wd + wr + wt;
+  if (sum <= 0.0f) return true;
+  float xi = rand01(&rng) * sum;
+  float3 nd, wc;
+  if (xi < wd) {
+    float pc = wd / sum;
+    float z = rand01(&rng) * 2.0f - 1.0f;
+    float t = rand01(&rng) * 2.0f * CUDART_PI_F;
+    float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+    nd = add(v3(r * cosf(t), r * sinf(t), z), n);
+    wc = divs(cd, pc);
+  } else if (xi < wd + wr) {
+    float pc = wr / sum;
+    nd = reflect_dir(n, inc);
+    wc = divs(cr, pc);
+  } else {
+    float pc = wt / sum;
+    nd = refract_dir(inc, n, m0.w);
+    wc = divs(ct, pc);
+  }
+  o = add(pos, mul(nd, kEps));
+  thr = mulv(thr, wc);
+  d = nd;
+  depth++;
+  return depth >= max_depth;
+}
+
+// The camera ray of sample `so` of pixel (x, y) and its random stream (renderKernel
+// prologue, K:1251-1264).
+__device__ __forceinline__ void camera_sample(const RenderArgs& a, int x, int y, int so,
+                                              uint32_t base_seed, uint32_t& rng, float3& o,
+                                              float3& d) {
+  uint32_t seed = base_seed ^ hash_u32((uint32_t)so);
+  seed ^= hash_u32((uint32_t)(so * 0x9E3779B9u));
+  rng = hash_u32(seed);
+  const float aspect = (float)a.width / (float)a.height;
+  float jx = rand01(&rng) - 0.5f;
+  float jy = rand01(&rng) - 0.5f;
+  float u = ((((float)x + 0.5f) + jx) * (2.0f / (float)a.width) - 1.0f) * aspect;
+  float v = 1.0f - ((((float)y + 0.5f) + jy) * (2.0f / (float)a.height));
+  o = a.cam_pos;
+  d = add(add(a.cam_f, mul(a.cam_r, u)), mul(a.cam_u, v));
+}
+
 // SDEPTH traversal-stack entries per thread in shared memory (16 KB a block at 16), for
 // scenes far larger than the caches: there the local-memory stack's lines compete with the
 // scene for L1 and L2.  A scene that the caches hold keeps the whole stack in local memory
@@ -86,7 +156,6 @@ __global__ void __launch_bounds__(128, RTB_RENDER_BLOCKS_PER_SM) k_render(Render
   int depth = 0;
   bool path = false;
   bool done = false;
-  const float aspect = (float)a.width / (float)a.height;
   while (true) {
     // ---- fetch a pixel (warp-aggregated) for lanes that need one
     bool need = !done && pixel < 0;
@@ -123,15 +192,7 @@ __global__ void __launch_bounds__(128, RTB_RENDER_BLOCKS_PER_SM) k_render(Render
     if (__all_sync(0xFFFFFFFFu, done)) break;
     // ---- start a sample (renderKernel prologue, K:1251-1264)
     if (!done && !path) {
-      uint32_t seed = base_seed ^ hash_u32((uint32_t)so);
-      seed ^= hash_u32((uint32_t)(so * 0x9E3779B9u));
-      rng = hash_u32(seed);
-      float jx = rand01(&rng) - 0.5f;
-      float jy = rand01(&rng) - 0.5f;
-      float u = ((((float)x + 0.5f) + jx) * (2.0f / (float)a.width) - 1.0f) * aspect;
-      float v = 1.0f - ((((float)y + 0.5f) + jy) * (2.0f / (float)a.height));
-      o = a.cam_pos;
-      d = add(add(a.cam_f, mul(a.cam_r, u)), mul(a.cam_u, v));
+      camera_sample(a, x, y, so, base_seed, rng, o, d);
       thr = v3(1.0f, 1.0f, 1.0f);
       rad = v3(0.0f, 0.0f, 0.0f);
       depth = 0;
@@ -145,54 +206,7 @@ __global__ void __launch_bounds__(128, RTB_RENDER_BLOCKS_PER_SM) k_render(Render
                                                   &s_stack[0][threadIdx.x]);
     if (tracing) {
       if (METRICS) rays++;
-      if (!hit) {
-        rad = add(rad, mulv(thr, S.background));
-        finished = true;
-      } else {
-        float3 pos, n;
-        int mi;
-        hit_record(S, b, o, d, &pos, &n, &mi);
-        float4 m0 = make_float4(0, 0, 0, 0), m1 = m0, m2 = m0, m3 = m0;
-        if (mi >= 0) {
-          const float4* mp = S.materials + 4 * mi;
-          m0 = __ldg(mp);
-          m1 = __ldg(mp + 1);
-          m2 = __ldg(mp + 2);
-          m3 = __ldg(mp + 3);
-        }
-        float3 cd = v3(m0.x, m0.y, m0.z), cr = v3(m1.x, m1.y, m1.z), ct = v3(m2.x, m2.y, m2.z);
-        rad = add(rad, mulv(thr, v3(m3.x, m3.y, m3.z)));
-        float3 inc = neg(d);
-        float wd = luminance(cd), wr = luminance(cr), wt = luminance(ct);
-        float sum = wd + wr + wt;
-        if (sum <= 0.0f) {
-          finished = true;
-        } else {
-          float xi = rand01(&rng) * sum;
-          float3 nd, wc;
-          if (xi < wd) {
-            float pc = wd / sum;
-            float z = rand01(&rng) * 2.0f - 1.0f;
-            float t = rand01(&rng) * 2.0f * CUDART_PI_F;
-            float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
-            nd = add(v3(r * cosf(t), r * sinf(t), z), n);
-            wc = divs(cd, pc);
-          } else if (xi < wd + wr) {
-            float pc = wr / sum;
-            nd = reflect_dir(n, inc);
-            wc = divs(cr, pc);
-          } else {
-            float pc = wt / sum;
-            nd = refract_dir(inc, n, m0.w);
-            wc = divs(ct, pc);
-          }
-          o = add(pos, mul(nd, kEps));
-          thr = mulv(thr, wc);
-          d = nd;
-          depth++;
-          if (depth >= a.max_depth) finished = true;
-        }
-      }
+      finished = shade_segment(S, hit, b, o, d, thr, rad, rng, depth, a.max_depth);
     }
     if (finished && titem >= 0) {
       path = false;
@@ -310,6 +324,119 @@ constexpr int kSharedStackDepth = 16;
 // At most 64M tail samples (768 MB of radiance, held by the context); frames whose last
 // four pixels per resident thread hold more samples split fewer pixels.
 constexpr long long kMaxTailItems = 1LL << 26;
+
+// ---- the wavefront form of a frame (rtb_render_device_wavefront)
+//
+// One wave per sample index over every pixel of the frame; per bounce, k_wf_trace runs the
+// closest-hit query of every live path of the wave (the compacted list) and k_wf_shade
+// shades it through the same shade_segment as k_render, appending the paths that go on to
+// the next list.  Path state lives in HBM, 16-byte records per path: origin, direction,
+// throughput with the random stream's state, radiance with the depth, and the hit.  A
+// pixel's samples are summed in sample order, one wave after the other, as k_render sums
+// them, so the image is bit-identical.  It exists as the A/B counterpart of the persistent
+// kernel: on the B200 it is slower (the state round trips and the per-bounce launches cost
+// more than the warps' coherence buys).
+struct WaveState {
+  float4* o;    // origin (w unused)
+  float4* d;    // direction (w unused)
+  float4* thr;  // throughput; w holds the random stream's state
+  float4* rad;  // radiance; w holds the depth
+  Best* hit;
+  int* list[2];
+  int* count;   // sizes of list[0] and list[1]
+};
+
+__global__ void __launch_bounds__(256) k_wf_start(RenderArgs a, WaveState W, int so, int cur) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.pixels) return;
+  const int x = (int)(p % a.width), y = (int)(p / a.width);
+  if (p == 0) W.count[cur] = (a.max_depth > 0 && !abort_raised(a.abort_flag)) ? (int)a.pixels : 0;
+  if (a.max_depth <= 0) {  // a black sample, summed like k_render's
+    float* out = a.out + 3 * p;
+    float3 acc = so == 0 ? v3(0, 0, 0) : add(v3(out[0], out[1], out[2]), v3(0, 0, 0));
+    if (so + 1 == a.spp) acc = mul(acc, 1.0f / (float)a.spp);
+    out[0] = acc.x;
+    out[1] = acc.y;
+    out[2] = acc.z;
+    return;
+  }
+  uint32_t rng;
+  float3 o, d;
+  camera_sample(a, x, y, so,
+                pixel_base_seed(a.frame_seed, a.frame_index, (uint32_t)y * (uint32_t)a.width + (uint32_t)x),
+                rng, o, d);
+  W.o[p] = make_float4(o.x, o.y, o.z, 0.0f);
+  W.d[p] = make_float4(d.x, d.y, d.z, 0.0f);
+  W.thr[p] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(rng));
+  W.rad[p] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(0));
+  W.list[cur][p] = (int)p;
+}
+
+template <int SDEPTH>
+__global__ void __launch_bounds__(128, RTB_RENDER_BLOCKS_PER_SM) k_wf_trace(RenderArgs a, WaveState W,
+                                                                           int cur) {
+  __shared__ int2 s_stack[SDEPTH > 0 ? SDEPTH : 1][128];
+  const int n = W.count[cur];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if ((i & ~31) >= n) return;  // whole warps only: the traversal is warp-cooperative
+  const bool active = i < n;
+  const int p = active ? W.list[cur][i] : 0;
+  float3 o = v3(0, 0, 0), d = v3(0, 0, 0);
+  if (active) {
+    const float4 o4 = W.o[p], d4 = W.d[p];
+    o = v3(o4.x, o4.y, o4.z);
+    d = v3(d4.x, d4.y, d4.z);
+  }
+  Best b;
+  TraceCounters c{};
+  const bool hit = trace_closest<false, SDEPTH, 128>(a.S, o, d, active, b, &c, nullptr,
+                                                    &s_stack[0][threadIdx.x]);
+  if (active) {
+    if (!hit) b.type = -1;
+    W.hit[p] = b;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_wf_shade(RenderArgs a, WaveState W, int so, int cur) {
+  const int n = W.count[cur];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  if ((i & ~31) >= n) return;
+  bool more = false;
+  int p = 0;
+  if (i < n) {
+    p = W.list[cur][i];
+    const float4 o4 = W.o[p], d4 = W.d[p], t4 = W.thr[p], r4 = W.rad[p];
+    float3 o = v3(o4.x, o4.y, o4.z), d = v3(d4.x, d4.y, d4.z);
+    float3 thr = v3(t4.x, t4.y, t4.z), rad = v3(r4.x, r4.y, r4.z);
+    uint32_t rng = __float_as_uint(t4.w);
+    int depth = __float_as_int(r4.w);
+    const Best b = W.hit[p];
+    if (shade_segment(a.S, b.type >= 0, b, o, d, thr, rad, rng, depth, a.max_depth)) {
+      float* out = a.out + 3 * (size_t)p;
+      float3 acc = so == 0 ? rad : add(v3(out[0], out[1], out[2]), rad);
+      if (so + 1 == a.spp) acc = mul(acc, 1.0f / (float)a.spp);
+      out[0] = acc.x;
+      out[1] = acc.y;
+      out[2] = acc.z;
+    } else {
+      W.o[p] = make_float4(o.x, o.y, o.z, 0.0f);
+      W.d[p] = make_float4(d.x, d.y, d.z, 0.0f);
+      W.thr[p] = make_float4(thr.x, thr.y, thr.z, __uint_as_float(rng));
+      W.rad[p] = make_float4(rad.x, rad.y, rad.z, __int_as_float(depth));
+      more = true;
+    }
+  }
+  // warp-aggregated append to the next bounce's list
+  const unsigned m = __ballot_sync(0xFFFFFFFFu, more);
+  if (m) {
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(W.count + (cur ^ 1), __popc(m));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+    if (more) W.list[cur ^ 1][base + __popc(m & ((1u << lane) - 1u))] = p;
+  }
+}
 
 }  // namespace
 
@@ -499,6 +626,63 @@ rtb_status trace_rays(rtb_context* ctx, rtb_scene* scene, const float* d_rays, i
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "trace launch");
+  return RTB_OK;
+}
+
+rtb_status render_frame_wavefront(rtb_context* ctx, rtb_scene* scene, const rtb_camera* cam,
+                                  const rtb_render_params* p, float* d_rgb, cudaStream_t stream) {
+  FramePlan f;
+  rtb_status s = plan_frame(ctx, scene, cam, p, d_rgb, &f, 0, 1);
+  if (s != RTB_OK) return s;
+  if (f.metrics) return fail(ctx, RTB_ERR_UNSUPPORTED, "the wavefront form has no metrics build");
+  const long long P = f.a.pixels;
+  if (P > 0x7FFFFFFFLL) return fail(ctx, RTB_ERR_INVALID_ARGUMENT, "frame too large");
+  // path state: four 16-byte records, the hit and two list slots per pixel, two counts
+  const size_t bytes = (size_t)P * (4 * sizeof(float4) + sizeof(Best) + 2 * sizeof(int)) + 256;
+  if (bytes > ctx->wave_bytes) {
+    cudaStreamSynchronize(stream);  // an earlier wavefront frame may still use the buffer
+    cudaFree(ctx->d_wave);
+    ctx->d_wave = nullptr;
+    ctx->wave_bytes = 0;
+    if (cudaMalloc(&ctx->d_wave, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ctx, RTB_ERR_OUT_OF_MEMORY, "wavefront path state");
+    }
+    ctx->wave_bytes = bytes;
+  }
+  char* q = (char*)ctx->d_wave;
+  WaveState W;
+  W.o = (float4*)q;
+  W.d = W.o + P;
+  W.thr = W.d + P;
+  W.rad = W.thr + P;
+  W.hit = (Best*)(W.rad + P);
+  W.list[0] = (int*)(W.hit + P);
+  W.list[1] = W.list[0] + P;
+  W.count = W.list[1] + P;
+  f.a.abort_flag = ctx->d_abort;
+  const unsigned g256 = (unsigned)((P + 255) / 256), g128 = (unsigned)((P + 127) / 128);
+  int launches = 0;
+  for (int so = 0; so < f.a.spp; ++so) {
+    int cur = 0;
+    k_wf_start<<<g256, 256, 0, stream>>>(f.a, W, so, cur);
+    ++launches;
+    for (int b = 0; b < f.a.max_depth; ++b) {
+      if (f.shared_stack == kSharedStackDepth)
+        k_wf_trace<kSharedStackDepth><<<g128, 128, 0, stream>>>(f.a, W, cur);
+      else if (f.shared_stack == 8)
+        k_wf_trace<8><<<g128, 128, 0, stream>>>(f.a, W, cur);
+      else
+        k_wf_trace<0><<<g128, 128, 0, stream>>>(f.a, W, cur);
+      cudaMemsetAsync(W.count + (cur ^ 1), 0, sizeof(int), stream);
+      k_wf_shade<<<g256, 256, 0, stream>>>(f.a, W, so, cur);
+      launches += 2;
+      cur ^= 1;
+    }
+  }
+  ctx->render_launches = launches;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "wavefront launch");
   return RTB_OK;
 }
 

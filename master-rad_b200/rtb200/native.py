@@ -142,6 +142,8 @@ SIGNATURES = {
                                     C.POINTER(RenderParams), FP]),
     "rtb_render_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Camera),
                                     C.POINTER(RenderParams), C.c_void_p, C.c_void_p]),
+    "rtb_render_device_wavefront": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Camera),
+                                              C.POINTER(RenderParams), C.c_void_p, C.c_void_p]),
     "rtb_render_rows_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Camera),
                                          C.POINTER(RenderParams), C.c_int, C.c_int, C.c_void_p,
                                          C.c_void_p]),
