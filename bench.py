@@ -99,6 +99,9 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ref-kernel", action="store_true")
+    ap.add_argument("--form", default="persistent", choices=["persistent", "wavefront"],
+                    help="the timed frames' form: the persistent kernel (rtb_render_device) or "
+                         "the wavefront kernels (rtb_render_device_wavefront), bit-identical")
     ap.add_argument("--no-other-configs", action="store_true",
                     help="skip the other configurations measured after the headline line's timing")
     ap.add_argument("--split", default="rows", choices=["rows", "frames"],
@@ -501,16 +504,57 @@ def frames_measure(ctx, w, steps, warmup, flush, stream, ref_frames=0, sm_mhz=No
     return d
 
 
+def wavefront_measure(ctx, w, steps, warmup, flush, stream):
+    """The same frames in both forms: the persistent kernel (rtb_render_device) and the
+    wavefront kernels (rtb_render_device_wavefront); Msamples/s of each (CUDA events around
+    each frame, L2 flushed before each outside the events) and whether the images agree
+    bit for bit."""
+    import torch
+    res = ResidentScene.build(ctx, w.scene)
+    cam = camera_struct(w.camera)
+    sh = C.c_void_p(stream.cuda_stream)
+    imgs, vals = {}, {}
+    for form, fn in (("persistent", ctx.lib.rtb_render_device),
+                     ("wavefront", ctx.lib.rtb_render_device_wavefront)):
+        out = torch.empty(w.width * w.height * 3, dtype=torch.float32, device="cuda")
+        ms = []
+        for i in range(warmup + steps):
+            p = N.RenderParams(w.width, w.height, w.spp, w.max_depth, 3000 + i,
+                               w.frame_seed & 0xFFFFFFFFFFFFFFFF, 1, 0, 0)
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                ctx.check(fn(ctx.handle, res.handle, C.byref(cam), C.byref(p),
+                             C.c_void_p(out.data_ptr()), sh))
+                e1.record(stream)
+            e1.synchronize()
+            if i >= warmup:
+                ms.append(e0.elapsed_time(e1))
+        imgs[form] = out.cpu().numpy()
+        vals[form] = w.width * w.height * w.spp / (statistics.mean(ms) / 1e3) / 1e6
+    res.close()
+    return {"value": vals["wavefront"], "unit": "Msamples/s", "persistent_value": vals["persistent"],
+            "wavefront_over_persistent": vals["wavefront"] / vals["persistent"], "frames": steps,
+            "images_identical": bool(np.array_equal(imgs["wavefront"].view(np.int32),
+                                                    imgs["persistent"].view(np.int32))),
+            "frame": "%dx%d %dspp depth%d" % (w.width, w.height, w.spp, w.max_depth),
+            "form": "one wave per sample index; per bounce a trace and a shade kernel over the "
+                    "compacted live paths; path state in HBM"}
+
+
 def other_configs(ctx, local, flush, sm_mhz=None):
     """The benchmark's other configurations, measured once after the headline timing so that
     one default run shows them all: the plain 64-sphere frame (with the reference kernel
-    beside it), the 1M-primitive scene (device build and frames), the 64-scene batch with
+    beside it), the C2 frame in the wavefront form beside the persistent kernel, the
+    1M-primitive scene (device build and frames), the 64-scene batch with
     the default tuning (versus its scenes' frames back to back) and the differentiable
     configuration (forward, backward and the finite-difference check)."""
     import torch
     stream = torch.cuda.Stream(device=local)
     out = {}
     out["C1_plain"] = frames_measure(ctx, synth.plain_workload(), 10, 3, flush, stream, ref_frames=3)
+    out["C2_wavefront"] = wavefront_measure(ctx, synth.hetero_workload(), 2, 1, flush, stream)
     out["C3_scale"] = frames_measure(ctx, synth.scale_workload(), 2, 1, flush, stream,
                                      sm_mhz=sm_mhz)
     works = synth.batched_workloads()
@@ -723,10 +767,13 @@ def main():
         return N.RenderParams(w.width, w.height, w.spp, w.max_depth, frame,
                               w.frame_seed & 0xFFFFFFFFFFFFFFFF, 1, metrics, 0)
 
+    render_fn = (lib.rtb_render_device_wavefront if args.form == "wavefront"
+                 else lib.rtb_render_device)
+
     def render(frame, metrics=0):
         p = params(frame, metrics)
-        ctx.check(lib.rtb_render_device(ctx.handle, res.handle, C.byref(cam), C.byref(p),
-                                        C.c_void_p(out.data_ptr()), sh))
+        ctx.check(render_fn(ctx.handle, res.handle, C.byref(cam), C.byref(p),
+                            C.c_void_p(out.data_ptr()), sh))
 
     # ---- counters for the roofline: the kernel's metrics build on this rank's first frame
     #      (untimed; a host-buffer render fills rtb_frame_stats with the counters)
@@ -744,6 +791,8 @@ def main():
     # ---- a step: this rank's own frame, or (rows split) this rank's rows of one frame
     #      shared by all ranks followed by the all-gather of every rank's rows
     split_rows = world > 1 and args.split == "rows"
+    if split_rows and args.form == "wavefront":
+        raise SystemExit("--form wavefront renders whole frames: use --split frames")
     if split_rows:
         from rtb200 import split
         k_rows = split.band_rows(w.height, world)
@@ -879,6 +928,7 @@ def main():
                        "spp": w.spp, "max_depth": w.max_depth, "bvh": "weighted SAH leaf<=4 "
                        "(sphere 1.0, box 1.3, affine 2.1), device-built",
                        "l2": "flushed between frames (256 MiB write outside the events)",
+                       "form": args.form,
                        "parallelism": ("one frame per step, rows r, r+N, ... on rank r, "
                                        "NCCL all-gather of the rows" if split_rows else
                                        "frames per rank" if world > 1 else "single GPU")},

@@ -65,8 +65,10 @@ __device__ __forceinline__ uint32_t pixel_base_seed(unsigned long long frame_see
 
 // One path segment after its closest-hit query (tracePath loop body, K:1098-1162): the
 // background on a miss; else the hit's emission, the lobe chosen by luminance, and the
-// next ray with its throughput.  Returns true when the path ends.  Both frame forms (the
-// persistent k_render and the wavefront kernels) shade through this one function.
+// next ray with its throughput.  Returns true when the path ends.  The wavefront kernels
+// shade through this function; k_render keeps the same statements inline (as a function
+// they cost it 1.5-3.6 % of its speed), and the tests hold the two forms' frames equal bit
+// for bit.
 __device__ __forceinline__ bool shade_segment(const DevScene& S, bool hit, const Best& b, float3& o,
                                               float3& d, float3& thr, float3& rad, uint32_t& rng,
                                               int& depth, int max_depth) {
@@ -117,7 +119,7 @@ __device__ __forceinline__ bool shade_segment(const DevScene& S, bool hit, const
 }
 
 // The camera ray of sample `so` of pixel (x, y) and its random stream (renderKernel
-// prologue, K:1251-1264).
+// prologue, K:1251-1264), for the wavefront kernels (k_render's prologue is inline).
 __device__ __forceinline__ void camera_sample(const RenderArgs& a, int x, int y, int so,
                                               uint32_t base_seed, uint32_t& rng, float3& o,
                                               float3& d) {
@@ -156,6 +158,7 @@ __global__ void __launch_bounds__(128, RTB_RENDER_BLOCKS_PER_SM) k_render(Render
   int depth = 0;
   bool path = false;
   bool done = false;
+  const float aspect = (float)a.width / (float)a.height;
   while (true) {
     // ---- fetch a pixel (warp-aggregated) for lanes that need one
     bool need = !done && pixel < 0;
@@ -192,7 +195,15 @@ __global__ void __launch_bounds__(128, RTB_RENDER_BLOCKS_PER_SM) k_render(Render
     if (__all_sync(0xFFFFFFFFu, done)) break;
     // ---- start a sample (renderKernel prologue, K:1251-1264)
     if (!done && !path) {
-      camera_sample(a, x, y, so, base_seed, rng, o, d);
+      uint32_t seed = base_seed ^ hash_u32((uint32_t)so);
+      seed ^= hash_u32((uint32_t)(so * 0x9E3779B9u));
+      rng = hash_u32(seed);
+      float jx = rand01(&rng) - 0.5f;
+      float jy = rand01(&rng) - 0.5f;
+      float u = ((((float)x + 0.5f) + jx) * (2.0f / (float)a.width) - 1.0f) * aspect;
+      float v = 1.0f - ((((float)y + 0.5f) + jy) * (2.0f / (float)a.height));
+      o = a.cam_pos;
+      d = add(add(a.cam_f, mul(a.cam_r, u)), mul(a.cam_u, v));
       thr = v3(1.0f, 1.0f, 1.0f);
       rad = v3(0.0f, 0.0f, 0.0f);
       depth = 0;
@@ -206,7 +217,54 @@ __global__ void __launch_bounds__(128, RTB_RENDER_BLOCKS_PER_SM) k_render(Render
                                                   &s_stack[0][threadIdx.x]);
     if (tracing) {
       if (METRICS) rays++;
-      finished = shade_segment(S, hit, b, o, d, thr, rad, rng, depth, a.max_depth);
+      if (!hit) {
+        rad = add(rad, mulv(thr, S.background));
+        finished = true;
+      } else {
+        float3 pos, n;
+        int mi;
+        hit_record(S, b, o, d, &pos, &n, &mi);
+        float4 m0 = make_float4(0, 0, 0, 0), m1 = m0, m2 = m0, m3 = m0;
+        if (mi >= 0) {
+          const float4* mp = S.materials + 4 * mi;
+          m0 = __ldg(mp);
+          m1 = __ldg(mp + 1);
+          m2 = __ldg(mp + 2);
+          m3 = __ldg(mp + 3);
+        }
+        float3 cd = v3(m0.x, m0.y, m0.z), cr = v3(m1.x, m1.y, m1.z), ct = v3(m2.x, m2.y, m2.z);
+        rad = add(rad, mulv(thr, v3(m3.x, m3.y, m3.z)));
+        float3 inc = neg(d);
+        float wd = luminance(cd), wr = luminance(cr), wt = luminance(ct);
+        float sum = wd + wr + wt;
+        if (sum <= 0.0f) {
+          finished = true;
+        } else {
+          float xi = rand01(&rng) * sum;
+          float3 nd, wc;
+          if (xi < wd) {
+            float pc = wd / sum;
+            float z = rand01(&rng) * 2.0f - 1.0f;
+            float t = rand01(&rng) * 2.0f * CUDART_PI_F;
+            float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+            nd = add(v3(r * cosf(t), r * sinf(t), z), n);
+            wc = divs(cd, pc);
+          } else if (xi < wd + wr) {
+            float pc = wr / sum;
+            nd = reflect_dir(n, inc);
+            wc = divs(cr, pc);
+          } else {
+            float pc = wt / sum;
+            nd = refract_dir(inc, n, m0.w);
+            wc = divs(ct, pc);
+          }
+          o = add(pos, mul(nd, kEps));
+          thr = mulv(thr, wc);
+          d = nd;
+          depth++;
+          if (depth >= a.max_depth) finished = true;
+        }
+      }
     }
     if (finished && titem >= 0) {
       path = false;
@@ -329,8 +387,8 @@ constexpr long long kMaxTailItems = 1LL << 26;
 //
 // One wave per sample index over every pixel of the frame; per bounce, k_wf_trace runs the
 // closest-hit query of every live path of the wave (the compacted list) and k_wf_shade
-// shades it through the same shade_segment as k_render, appending the paths that go on to
-// the next list.  Path state lives in HBM, 16-byte records per path: origin, direction,
+// shades it through shade_segment (k_render's segment statements), appending the paths
+// that go on to the next list.  Path state lives in HBM, 16-byte records per path: origin, direction,
 // throughput with the random stream's state, radiance with the depth, and the hit.  A
 // pixel's samples are summed in sample order, one wave after the other, as k_render sums
 // them, so the image is bit-identical.  It exists as the A/B counterpart of the persistent
