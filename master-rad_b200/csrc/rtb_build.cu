@@ -623,9 +623,12 @@ struct SubtreeSmem {
   double lw[kSubtreeSize];
   unsigned char lside[kSubtreeSize];
   int idx[3][kSubtreeSize];     // the subtree's three axis orders (slots)
-  double sterm[3][kSubtreeSize];  // per axis: suffix area x suffix weight of the current node
-  int tmp[3][kSubtreeSize];     // per axis: partition scratch
-  int stack[kSubtreeSize];      // pending nodes (depth first)
+  union {  // the sweeps' terms, then (the sweeps done) the partition's scratch
+    double sterm[3][kSubtreeSize];  // per axis: suffix area x suffix weight of the current node
+    int tmp[3][kSubtreeSize];       // per axis: partition scratch
+  };
+  int4 stack[kSubtreeSize];     // pending nodes, depth first: node, start, end,
+                                // depth << 2 | (order axis + 1)
   double best_cost[3];
   long long best_flat[3];
   int sp, child;
@@ -711,7 +714,7 @@ __global__ void __launch_bounds__(kSubtreeThreads, RTB_SUBTREE_BLOCKS_PER_SM) k_
   for (int a = 1; a < 3; ++a)
     for (int i = threadIdx.x; i < M; i += kSubtreeThreads) sm.idx[a][i] = slot_of[I.a[a][rs + i]];
   if (threadIdx.x == 0) {
-    sm.stack[0] = root;
+    sm.stack[0] = make_int4(root, rs, re, (N.depth[root] << 2) | (N.order_axis[root] + 1));
     sm.sp = 1;
   }
   // the subtree's statistics, kept by thread 0 and added to the build's once at the end
@@ -719,15 +722,18 @@ __global__ void __launch_bounds__(kSubtreeThreads, RTB_SUBTREE_BLOCKS_PER_SM) k_
   int leaves = 0, min_occ = 0x7FFFFFFF, max_occ = 0, max_depth = 0;
   __syncthreads();
   while (sm.sp > 0) {
-    const int node = sm.stack[sm.sp - 1];
+    const int4 en = sm.stack[sm.sp - 1];
     __syncthreads();
     if (threadIdx.x == 0) sm.sp--;
-    const int s = N.start[node], e = N.end[node], m = e - s, lo = s - rs;
-    const int oa = N.order_axis[node];
-    // node bounds (every warp computes the same union)
+    const int node = en.x, s = en.y, e = en.z, m = e - s, lo = s - rs;
+    const int oa = (en.w & 3) - 1, depth = en.w >> 2;
+    // node bounds (every warp computes the same union): a butterfly over the lanes that hold
+    // positions, then lane 0's union to all
     Box nb = empty_box();
     for (int i = lane; i < m; i += 32) nb = BoxUnion()(nb, sm.lbox[sm.idx[0][lo + i]]);
-    for (int off = 16; off > 0; off >>= 1) {
+    int span = 1;
+    while (span < min(m, 32)) span <<= 1;
+    for (int off = 1; off < span; off <<= 1) {
       Box o;
       for (int k = 0; k < 3; ++k) {
         o.mn[k] = __shfl_xor_sync(0xFFFFFFFFu, nb.mn[k], off);
@@ -735,6 +741,7 @@ __global__ void __launch_bounds__(kSubtreeThreads, RTB_SUBTREE_BLOCKS_PER_SM) k_
       }
       nb = BoxUnion()(nb, o);
     }
+    if (span < 32) nb = warp_bcast(nb, 0);
     const double node_a = surface_area(nb) * traversal;
     // this warp's axis
     double best = CUDART_INF;
@@ -817,7 +824,7 @@ __global__ void __launch_bounds__(kSubtreeThreads, RTB_SUBTREE_BLOCKS_PER_SM) k_
         leaves++;
         min_occ = min(min_occ, m);
         max_occ = max(max_occ, m);
-        max_depth = max(max_depth, N.depth[node]);
+        max_depth = max(max_depth, depth);
       }
       __syncthreads();
       continue;
@@ -835,10 +842,11 @@ __global__ void __launch_bounds__(kSubtreeThreads, RTB_SUBTREE_BLOCKS_PER_SM) k_
       N.start[r] = s + pos;
       N.end[r] = e;
       N.order_axis[l] = N.order_axis[r] = axis;
-      N.depth[l] = N.depth[r] = N.depth[node] + 1;
+      N.depth[l] = N.depth[r] = depth + 1;
       N.leaf[l] = N.leaf[r] = 0;
-      sm.stack[sm.sp] = r;
-      sm.stack[sm.sp + 1] = l;
+      const int meta = ((depth + 1) << 2) | (axis + 1);
+      sm.stack[sm.sp] = make_int4(r, s + pos, e, meta);
+      sm.stack[sm.sp + 1] = make_int4(l, s, s + pos, meta);
       sm.sp += 2;
     }
     // stable partition of the other two axis orders by side
