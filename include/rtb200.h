@@ -210,8 +210,9 @@ RTB_API rtb_status rtb_render_device(rtb_context* ctx, rtb_scene* scene, const r
  * the wave and one shades them (path state in device memory, held by the context and grown
  * to the largest frame).  The A/B counterpart of the persistent kernel behind
  * rtb_render_device, which is faster on the B200; no metrics build (RTB_ERR_UNSUPPORTED).
- * No counterpart in the reference, whose renderKernel is one thread per pixel
- * (GpuKernelSources.java:1167-1315). */
+ * rtb_request_abort stops it at the start of the next wave (sample index), leaving the
+ * frame unfinished.  No counterpart in the reference, whose renderKernel is one thread per
+ * pixel (GpuKernelSources.java:1167-1315). */
 RTB_API rtb_status rtb_render_device_wavefront(rtb_context* ctx, rtb_scene* scene,
                                                const rtb_camera* camera,
                                                const rtb_render_params* params,
