@@ -140,7 +140,7 @@ __device__ __forceinline__ void camera_sample(const RenderArgs& a, int x, int y,
 // scene for L1 and L2.  A scene that the caches hold keeps the whole stack in local memory
 // and the caches for itself.
 #ifndef RTB_RENDER_BLOCKS_PER_SM
-#define RTB_RENDER_BLOCKS_PER_SM 8  // 64 registers a thread; 7 and 6 measured slower
+#define RTB_RENDER_BLOCKS_PER_SM 8  // 64 registers a thread; 6, 7 and 9 measured slower
 #endif
 template <bool METRICS, int SDEPTH>
 __global__ void __launch_bounds__(128, RTB_RENDER_BLOCKS_PER_SM) k_render(RenderArgs a) {
