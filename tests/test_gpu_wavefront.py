@@ -52,6 +52,15 @@ def test_wavefront_frame_equals_the_persistent_kernel(ctx, kind, spp, depth):
     np.testing.assert_array_equal(a.view(np.int32), b.view(np.int32))
 
 
+@pytest.mark.parametrize("width,height", [(1, 1), (7, 3), (33, 5)])
+def test_wavefront_odd_frame_sizes(ctx, width, height):
+    """Frames smaller than a warp or a block, and sizes that are not multiples of either."""
+    w = synth.hetero_workload(width=width, height=height, spp=5, depth=6)
+    (s0, a), (s1, b) = _frames(ctx, w, 5, 6)
+    assert s0 == 0 and s1 == 0
+    np.testing.assert_array_equal(a.view(np.int32), b.view(np.int32))
+
+
 def test_wavefront_refuses_the_metrics_build(ctx):
     w = synth.plain_workload()
     (_, _), (st, _) = _frames(ctx, w, 1, 2, metrics=1)
