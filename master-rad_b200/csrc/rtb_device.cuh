@@ -526,10 +526,13 @@ __device__ bool trace_closest(const DevScene& S, float3 o, float3 d, bool active
     int qfirst0 = 0, qmeta0 = 0, qfirst1 = 0, qmeta1 = 0;
     int npend = 0;
     bool pend = false;  // this lane cannot take another leaf pair
-    while (__any_sync(0xFFFFFFFFu, node >= 0 || npend > 0)) {
+    while (true) {
       pend = npend >= 2;
-      if (__popc(__ballot_sync(0xFFFFFFFFu, node >= 0 && !pend)) <= kLeafPostponeLanes &&
-          __any_sync(0xFFFFFFFFu, npend > 0)) {
+      // lanes that can walk, lanes with recorded leaves (a lane that cannot walk has some)
+      const unsigned walk = __ballot_sync(0xFFFFFFFFu, node >= 0 && !pend);
+      const unsigned waiting = __ballot_sync(0xFFFFFFFFu, npend > 0);
+      if ((walk | waiting) == 0u) break;
+      if (__popc(walk) <= kLeafPostponeLanes && waiting != 0u) {
         int c0 = npend >= 1 ? (pmeta0 & 0xFFFFFF) : 0, c1 = npend >= 1 ? (pmeta1 & 0xFFFFFF) : 0;
         int c2 = npend >= 2 ? (qmeta0 & 0xFFFFFF) : 0, c3 = npend >= 2 ? (qmeta1 & 0xFFFFFF) : 0;
         int e1 = c0 + c1, e2 = e1 + c2, e3 = e2 + c3;
