@@ -60,16 +60,16 @@ FALLBACK_HBM_GBS = 6650.0
 # (profiles/k_render_scale1M_480x270x4spp_full.md); workloads without a capture report
 # null traffic.
 CAPTURE_FRAME = {"hetero": "1024x768x4spp", "scale": "480x270x4spp"}
-TRAFFIC_BYTES_PER_SAMPLE = {"hetero": (26.58e6 + 143.07e6) / 3145728,
+TRAFFIC_BYTES_PER_SAMPLE = {"hetero": (23.57e6 + 143.13e6) / 3145728,
                             "scale": (359.48e6 + 153.86e6) / 518400}
-# smsp__inst_executed.sum of k_render per sample from the same captures (8.862 G warp
+# smsp__inst_executed.sum of k_render per sample from the same captures (8.899 G warp
 # instructions for 3,145,728 samples; 2.823 G for 518,400), for the issue bound: warp
 # instructions per second against one instruction per cycle on each of the 4 schedulers of
 # every SM.
-INST_PER_SAMPLE = {"hetero": 8.862e9 / 3145728, "scale": 2.8227e9 / 518400}
+INST_PER_SAMPLE = {"hetero": 8.8986e9 / 3145728, "scale": 2.8227e9 / 518400}
 # smsp__thread_inst_executed_per_inst_executed of the same captures: active lanes per warp
 # instruction, which scales the issue bound to lane-instructions doing useful work.
-LANES_PER_INST = {"hetero": 9.22, "scale": 9.48}
+LANES_PER_INST = {"hetero": 9.30, "scale": 9.48}
 
 
 def issue_roofline(workload, samples, launch_ms, sm_count, sm_mhz):
